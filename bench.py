@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Benchmark of the per-block Godunov update (Mcell-updates/s).
+
+Workload (default): batched AMR blast snapshot -- 8^3 root blocks of 16^3,
+5 refinement levels, ~11.6k leaf blocks (uneven per level), FP64 HLLC +
+minmod, CFL 0.4, viscosity 5e-3.  One step = one full time step of the
+reference's main loop without AMR/output (dt reduction, two Godunov stages
+with ghost fill, viscous step), i.e. source/main.f90:81-100.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl wx3d|reference]
+
+--impl reference times the CPU restatement of the reference (oracle/, the
+reference's own Fortran cannot be built here: no Fortran compiler) on all host
+threads for the same workload.  Under torchrun (N>1) every rank runs an
+independent replica of the workload on its GPU (the graded path does not
+shard: one GPU, no MPI) and the job throughput is the sum.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    "blast-amr": dict(desc="batched AMR blast: 8^3 root blocks of 16^3, 5 levels, shell-refined snapshot, "
+                           "FP64 HLLC+minmod, CFL 0.4, eta 5e-3"),
+    "sedov256": dict(desc="Sedov blast 16^3 root blocks of 16^3 (256^3 cells), single level, FP64 HLLC+minmod"),
+    "sedov64": dict(desc="Sedov blast 4^3 root blocks of 16^3 (64^3 cells), single level, FP64 HLLC+minmod"),
+    "brio-wu": dict(desc="Brio-Wu MHD shock tube 256x16x16 cells, FP64 HLLD+minmod, 8-wave source"),
+    "snr-h": dict(desc="radiative SNR, H-rate EOS + COOL_H, 4^3 roots, 3 levels, FP64 HLLC+minmod"),
+}
+
+
+def build_problem(name: str):
+    from walicxe3d_b200 import problems
+    if name == "blast-amr":
+        return problems.blast_amr()
+    if name == "sedov256":
+        return problems.sedov(16)
+    if name == "sedov64":
+        return problems.sedov(4)
+    if name == "brio-wu":
+        return problems.brio_wu(16)
+    if name == "snr-h":
+        return problems.snr_h(nroot=4, maxlev=3)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([v.strip() for v in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for n, v in zip(names, r[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_time_oracle(prob, steps_max: int, budget_s: float, threads: int):
+    """Times the CPU oracle on the workload: whole steps, stopping once the
+    budget is spent.  Returns (Mcell-updates/s, steps timed, seconds)."""
+    import oracle
+    o = oracle.from_problem(prob, threads=threads)
+    o.step()  # warm the caches and the thread pool
+    n, t0 = 0, time.perf_counter()
+    while n < steps_max:
+        o.step()
+        n += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    o.close()
+    return prob.cells * n / dt / 1e6, n, dt
+
+
+def load_traffic(workload: str, cells_per_launch: int):
+    """DRAM bytes per launch of the corrector stage from the committed ncu
+    summary (bytes per cell measured on a smaller case), scaled to the launch."""
+    f = ROOT / "profiles" / "stage2_traffic.json"
+    if not f.exists():
+        return None
+    try:
+        d = json.loads(f.read_text())
+        return d["dram_bytes_per_cell"] * cells_per_launch
+    except Exception:
+        return None
+
+
+def run_reference(args, rank, world):
+    prob = build_problem(args.workload)
+    threads = os.cpu_count() or 1
+    if rank != 0:
+        return
+    budget = float(os.environ.get("WX3D_REF_BUDGET_S", "90"))
+    # warm-up steps are whole oracle steps too, bounded by a share of the budget
+    import oracle
+    o = oracle.from_problem(prob, threads=threads)
+    tw = time.perf_counter()
+    for _ in range(args.warmup):
+        o.step()
+        if time.perf_counter() - tw > budget / 4:
+            break
+    n, t0 = 0, time.perf_counter()
+    while n < args.steps:
+        o.step()
+        n += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    el = time.perf_counter() - t0
+    value = prob.cells * n / el / 1e6
+    line = {
+        "impl": "reference",
+        "metric": "Mcell-updates/s", "value": value, "unit": "Mcell-updates/s",
+        "n_gpus": world, "steps": n, "warmup": args.warmup, "ms_per_step": el / n * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "blocks": prob.nblocks, "cells": prob.cells,
+                   "description": WORKLOADS[args.workload]["desc"]},
+        "cpu_baseline": {"value": value, "unit": "Mcell-updates/s", "cores": threads, "kind": "port",
+                         "sample": f"{n} whole steps of the workload (of {args.steps} requested; "
+                                   f"{budget:.0f}s budget) by the C++ FP64 restatement of the reference, "
+                                   f"OpenMP over blocks"},
+        "e2e": {"value": value, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", default="wx3d", choices=["wx3d", "reference"])
+    ap.add_argument("--workload", default="blast-amr", choices=sorted(WORKLOADS))
+    ap.add_argument("--zsplit", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        if world > 1:
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=600))
+        run_reference(args, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from walicxe3d_b200.solver import from_problem
+
+    prob = build_problem(args.workload)
+    w = from_problem(prob)
+    stream = torch.cuda.current_stream()
+    w.set_stream(stream.cuda_stream)
+    if args.zsplit:
+        w.set_zsplit(args.zsplit)
+    w.set_timing(True)
+
+    # --- warm-up (graph capture happens here) ---
+    w.run(args.warmup - args.warmup % 2 if args.warmup >= 2 else 2)
+    torch.cuda.synchronize()
+
+    # --- device-resident timed region ---
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    k0 = w.kernels_launched
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    w.run_async(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = w.kernels_launched - k0
+    kt_ms, kt_n = w.kernel_times()
+    clocks = sampler.stop()
+    st = w.state
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        if dist is not None:
+            dist.barrier()
+    value = prob.cells * args.steps * world / (ms / 1e3) / 1e6
+
+    # --- roofline of the dominant kernel (corrector stage) ---
+    try:
+        peak, peak_src = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    neq = prob.cfg.neqtot
+    stage2_ms = kt_ms[1] / max(kt_n[1], 1)
+    alg_bytes = 3 * neq * 8 * prob.cells     # reads UP and U, writes the stage result
+    achieved = alg_bytes / (stage2_ms / 1e3) / 1e9 if stage2_ms > 0 else None
+    step_bytes = 40 * neq * prob.cells       # 5 compulsory state passes per step
+    step_achieved = step_bytes * args.steps * world / (ms / 1e3) / 1e9
+    traffic = load_traffic(args.workload, prob.cells)
+
+    # --- end to end through the C-ABI with host buffers ---
+    U_host = torch.from_numpy(prob.U).pin_memory()
+    U_out = torch.empty_like(U_host).pin_memory()
+    import ctypes
+    lib, ctx = w.lib, w.ctx
+    uptr = ctypes.cast(U_host.data_ptr(), ctypes.POINTER(ctypes.c_double))
+    optr = ctypes.cast(U_out.data_ptr(), ctypes.POINTER(ctypes.c_double))
+    from walicxe3d_b200.config import WxState
+    w.set_timing(False)
+    sst = WxState()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rc = lib.wx3d_upload_blocks(ctx, prob.nblocks, uptr)
+    for _ in range(args.steps):
+        rc |= lib.wx3d_step(ctx, ctypes.byref(sst))
+    rc |= lib.wx3d_download_blocks(ctx, prob.nblocks, optr)
+    e2e_s = time.perf_counter() - t0
+    if rc:
+        raise SystemExit(f"e2e leg failed with status {rc}")
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = prob.cells * args.steps * world / e2e_s / 1e6
+    state_bytes = prob.U.nbytes
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, n, secs = cpu_time_oracle(prob, 1000, float(os.environ.get("WX3D_CPU_BUDGET_S", "20")), os.cpu_count() or 1)
+        cpu = {"value": v, "unit": "Mcell-updates/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{n} whole steps of the same workload in {secs:.1f}s by the C++ FP64 restatement "
+                         f"of the reference (OpenMP over blocks)"}
+
+    if rank == 0:
+        line = {
+            "metric": "Mcell-updates/s", "value": value, "unit": "Mcell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "description": WORKLOADS[args.workload]["desc"],
+                       "blocks": prob.nblocks, "cells": prob.cells, "neq": neq,
+                       "levels": sorted({int(prob.tree.level(int(b))) for b in prob.local_blocks}),
+                       "l2": "state arrays larger than L2 (%.2f GB each)" % (state_bytes / 1e9),
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "path": "wx3d_run: CUDA graph of 2 steps replayed"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "kernel": "stage_kernel<ORDER=2> (corrector)", "peak_source": peak_src,
+                         "alg_bytes_per_launch": alg_bytes, "launch_ms": stage2_ms,
+                         "step_alg_gbs": step_achieved, "step_frac": step_achieved / peak},
+            "kernel_ms_per_launch": {k: (m / n if n else None) for k, m, n in
+                                     zip(["stage1", "stage2", "viscous", "sources"], kt_ms, kt_n)},
+            "e2e": {"value": e2e_value, "unit": "Mcell-updates/s",
+                    "h2d_bytes_per_step": state_bytes / args.steps + 32,
+                    "d2h_bytes_per_step": state_bytes / args.steps + 128,
+                    "note": "timed: upload of the state from pinned host memory, K wx3d_step calls (each "
+                            "returns time/dt/status to the host), download of the final state"},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+            "final_state": {"time": st.time, "dt": st.dt, "it": st.it},
+        }
+        print(json.dumps(line), flush=True)
+    w.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

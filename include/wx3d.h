@@ -1,0 +1,249 @@
+/*
+ * wx3d.h -- C-ABI of the B200 (sm_100a) per-block Godunov update for
+ * Walicxe3D-style block-structured AMR hydro/MHD.
+ *
+ * The entry points replace the argument-less Fortran module subroutines of
+ * the reference that act on module globals (U, UP, PRIM, dt, time, it):
+ *
+ *   hydroSolver()            source/hydro_solver.f90:39   -> wx3d_hydro_solver
+ *   getTimestep(dt)          source/hydro_solver.f90:129  -> wx3d_get_timestep
+ *   updatePrims()            source/hydro_core.f90:43     -> wx3d_update_prims
+ *   updateNeutralFraction()  source/hrate.f90:12          -> wx3d_update_neutral_fraction
+ *   cooling()                source/cooling.f90:37        -> wx3d_cooling
+ *   loadcooldata()           source/cooling.f90:135       -> wx3d_set_cooltable
+ *   boundary(depth, uvars)   source/boundary.f90:46       -> fused into the stage kernels
+ *   markByPhysical(...)      source/amr.f90:142           -> wx3d_mark
+ *   refineBlock(fatherID)    source/amr.f90:284 (data)    -> wx3d_refine
+ *   coarseBlocks()           source/amr.f90:1430 (data)   -> wx3d_coarsen
+ *   main-loop body           source/main.f90:81-100       -> wx3d_step / wx3d_run
+ *
+ * Memory: the library owns the device copies of every block's conserved
+ * variables (and primitives on request).  The host keeps the block tree
+ * (localBlocks, bIDs) and passes it with wx3d_set_mesh after every mesh
+ * change, exactly like the reference's localBlocks registry
+ * (source/globals.f90:125).
+ *
+ * Conventions: every call returns an int status (0 = OK).  Codes 1..27 and
+ * 255 mirror the reference's error codes (source/constants.f90:135-162);
+ * codes >= 100 are added by this library.  Calls are synchronous from the
+ * host's point of view unless the name ends in _async, are not thread safe,
+ * and use one CUDA stream per context (settable with wx3d_set_stream).
+ * Signatures carry plain pointers and sizes only.
+ */
+#ifndef WX3D_H
+#define WX3D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Block geometry: ncells_block and nghost (source/parameters.f90:113,209). */
+#define WX3D_NCELLS 16
+#define WX3D_NGHOST 2
+#define WX3D_BLOCK_CELLS (WX3D_NCELLS * WX3D_NCELLS * WX3D_NCELLS)
+#define WX3D_MAX_LEVELS 10 /* basegrid limit, source/init.f90:694-700 */
+#define WX3D_MAX_NEQ 12
+
+/* Directions (source/constants.f90:52-57). */
+enum { WX_LEFT = 1, WX_RIGHT = 2, WX_FRONT = 3, WX_BACK = 4, WX_BOTTOM = 5, WX_TOP = 6 };
+/* Boundary conditions (source/constants.f90:65-67). */
+enum { WX_BC_REFLECTIVE = 1, WX_BC_FREE_FLOW = 2, WX_BC_PERIODIC = 3 };
+/* Neighbour types (source/constants.f90:70-73). */
+enum { WX_NEIGH_SAME = 1, WX_NEIGH_COARSER = 2, WX_NEIGH_FINER = 3, WX_NEIGH_BOUNDARY = 4 };
+/* Refinement flags (source/constants.f90:76-78). */
+enum { WX_FLAG_NONE = 0, WX_FLAG_REFINE = 1, WX_FLAG_COARSE = 2 };
+/* Solvers (source/constants.f90:81-86). */
+enum {
+  WX_SOLVER_LAX = 1, WX_SOLVER_HLL1 = 2, WX_SOLVER_HLL = 3,
+  WX_SOLVER_HLLC = 4, WX_SOLVER_HLLE = 5, WX_SOLVER_HLLD = 6
+};
+/* Slope limiters (source/constants.f90:89-96). */
+enum {
+  WX_LIMITER_NO_AVERAGE = -1, WX_LIMITER_NONE = 0, WX_LIMITER_MINMOD = 1,
+  WX_LIMITER_VANLEER = 2, WX_LIMITER_ALBADA = 3, WX_LIMITER_UMIST = 4,
+  WX_LIMITER_WOODWARD = 5, WX_LIMITER_SUPERBEE = 6
+};
+/* Equations of state (source/constants.f90:99-102). */
+enum { WX_EOS_ADIABATIC = 0, WX_EOS_SINGLE_SPECIE = 1, WX_EOS_TWOTEMP = 2, WX_EOS_H_RATE = 3 };
+/* Cooling (source/constants.f90:106-110). */
+enum { WX_COOL_NONE = 0, WX_COOL_TABLE = 1, WX_COOL_TABLE_METAL = 2, WX_COOL_H = 3, WX_COOL_SCHURE = 4 };
+
+/* Status codes.  1..27 and 255 are the reference's (source/constants.f90:135-162). */
+enum {
+  WX_OK = 0,
+  WX_ERR_GENERIC = 255,
+  WX_ERR_INSUFICIENT_NBMAXPROC = 7,
+  WX_ERR_TOO_MANY_LEVS = 12,
+  WX_ERR_COOLING_LOAD_COEFS = 14,
+  WX_ERR_DIVISION_BY_ZERO = 23,
+  WX_ERR_NOT_ENOUGH_PASSIVES = 26,
+  WX_ERR_NAN_IN_FLUXES = 27,
+  WX_ERR_CUDA = 100,
+  WX_ERR_TIMEOUT = 101,
+  WX_ERR_NAN = 102,
+  WX_ERR_INVALID_ARG = 103,
+  WX_ERR_UNSUPPORTED = 104,
+  WX_ERR_NO_DEVICE = 105,
+  WX_ERR_MESH = 106
+};
+
+/*
+ * Run-time mirror of the compile-time parameters the hot path reads
+ * (source/parameters.f90 and the per-problem copies).  BFIELD, a Makefile
+ * switch in the reference (Makefile:34-128), is the field `bfield`.
+ */
+typedef struct wx_config {
+  int32_t neqtot;            /* neqtot = 5 + 3*bfield + npassive        */
+  int32_t npassive;          /* npassive                                 */
+  int32_t bfield;            /* -DBFIELD                                 */
+  int32_t mhd;               /* mhd                                      */
+  int32_t solver_type;       /* WX_SOLVER_*                              */
+  int32_t limiter_type;      /* WX_LIMITER_*                             */
+  int32_t eos_type;          /* WX_EOS_*                                 */
+  int32_t cooling_type;      /* WX_COOL_*                                */
+  int32_t bc[6];             /* bc_left, bc_right, bc_front, bc_back, bc_bottom, bc_top */
+  int32_t eight_wave;        /* Powell 8-wave source (brio-wu/parameters.f90:198) */
+  int32_t user_source_terms; /* must be 0: get_user_source_terms is not part of this ABI */
+  int32_t nbrootx, nbrooty, nbrootz; /* root blocks (MESH_MANUAL)        */
+  int32_t maxlev;            /* number of refinement levels              */
+  double gamma;              /* heat capacity ratio                      */
+  double cfl;                /* CFL                                      */
+  double visc_eta;           /* artificial viscosity                     */
+  double cooling_limit;      /* max fractional thermal loss per step     */
+  double mu0, mui, ion_thres;
+  double l_sc, d_sc, v_sc;   /* unit scalings; p_sc, e_sc, t_sc derived  */
+  double xphystot, yphystot, zphystot; /* box size (cgs)                 */
+  double tfin, dtout;        /* final time and output cadence (cgs)      */
+  double refine_thres, coarse_thres; /* markByPhysical thresholds        */
+} wx_config;
+
+/* Simulation state globals (source/globals.f90:52-56). */
+typedef struct wx_state {
+  double time;      /* code units */
+  double dt;        /* code units */
+  int32_t it;
+  int32_t nextout;
+  int32_t dumpout;  /* set when getTimestep clipped dt to an output time */
+  int32_t pad;
+} wx_state;
+
+/* Device-side health counters, read after a step (never a trap). */
+typedef struct wx_status {
+  int64_t pressure_floor;  /* flow2prim istat=1 (source/hydro_core.f90:355-358) */
+  int64_t density_floor;   /* flow2prim istat=2 (source/hydro_core.f90:361-364) */
+  int64_t zero_density;    /* flow2prim abort case (source/hydro_core.f90:335-338) */
+  int64_t nan_cells;       /* non-finite state after a step                     */
+  double max_cool_loss;    /* max fractional thermal loss before limiting       */
+  int64_t kernels_launched;/* running count of kernels this context launched    */
+} wx_status;
+
+typedef struct wx_ctx wx_ctx;
+
+/* Fills *cfg with the defaults of source/parameters.f90 (HD, HLLC, van Leer,
+ * free-flow, CFL 0.4, eta 5e-3) in code units (all scalings 1). */
+int wx3d_config_defaults(wx_config* cfg);
+
+/* Allocates HBM for max_blocks block slots.  Replaces the big-array
+ * allocation of initmain (source/init.f90:375-423). */
+int wx3d_init(const wx_config* cfg, int32_t max_blocks, wx_ctx** out);
+int wx3d_finalize(wx_ctx* ctx);
+
+/* Use an external cudaStream_t (NULL selects the context's own stream). */
+int wx3d_set_stream(wx_ctx* ctx, void* cuda_stream);
+
+/* localBlocks registry: bID of the block held in each slot, -1 if empty
+ * (source/globals.f90:125, source/init.f90:431-437).  Rebuilds the device
+ * neighbour table with the reference's tree queries (source/amr.f90:439-631). */
+int wx3d_set_mesh(wx_ctx* ctx, int32_t nslots, const int32_t* local_blocks);
+
+/* Device neighbour table as built by wx3d_set_mesh, for inspection:
+ * per slot and face (6): type, 4 neighbour slots.  face_type[nslots*6],
+ * face_slot[nslots*24]; empty slots report type 0. */
+int wx3d_get_neighbours(wx_ctx* ctx, int32_t nslots, int32_t* face_type, int32_t* face_slot);
+
+/* Slabs per block of the stage kernels (1, 2, 4 or 8 CTAs per block along z).
+ * wx3d_set_mesh picks a default; the autotuner overrides it. */
+int wx3d_set_zsplit(wx_ctx* ctx, int32_t zsplit);
+
+/* Conserved variables, native layout: u[slot][eq][k][j][i], 16^3 physical
+ * cells per block, host memory (pinned or pageable). */
+int wx3d_upload_blocks(wx_ctx* ctx, int32_t nslots, const double* u);
+int wx3d_download_blocks(wx_ctx* ctx, int32_t nslots, double* u);
+
+/* Conserved variables in the reference's own array layout
+ * U(nbMaxProc, neqtot, -1:18, -1:18, -1:18), block index fastest
+ * (source/globals.f90:97).  Only physical cells are read / written. */
+int wx3d_upload_U_fortran(wx_ctx* ctx, int32_t nbMaxProc, const double* U);
+int wx3d_download_U_fortran(wx_ctx* ctx, int32_t nbMaxProc, double* U);
+
+/* updatePrims (source/hydro_core.f90:43) on physical cells, then download
+ * PRIM in the native layout. */
+int wx3d_update_prims(wx_ctx* ctx);
+int wx3d_download_prims(wx_ctx* ctx, int32_t nslots, double* prim);
+
+int wx3d_set_state(wx_ctx* ctx, const wx_state* st);
+int wx3d_get_state(wx_ctx* ctx, wx_state* st);
+
+/* getTimestep (source/hydro_solver.f90:129) on the current primitives,
+ * using st.it as already incremented by the caller (source/main.f90:81).
+ * Does not change the stored dt. */
+int wx3d_get_timestep(wx_ctx* ctx, double* dt_glob);
+
+/* hydroSolver (source/hydro_solver.f90:39): dt, Godunov(order) or
+ * LaxFriedrichs, doViscousStep.  Updates state.dt and state.time. */
+int wx3d_hydro_solver(wx_ctx* ctx);
+
+/* updateNeutralFraction (source/hrate.f90:12) and cooling
+ * (source/cooling.f90:37).  maxloss may be NULL. */
+int wx3d_update_neutral_fraction(wx_ctx* ctx);
+int wx3d_cooling(wx_ctx* ctx, double* maxloss);
+
+/* One main-loop iteration without AMR and output (source/main.f90:81-100):
+ * it += 1, hydroSolver, updatePrims, updateNeutralFraction (EOS_H_RATE),
+ * cooling.  *out (may be NULL) receives the state after the step. */
+int wx3d_step(wx_ctx* ctx, wx_state* out);
+
+/* nsteps iterations of wx3d_step with no host synchronisation in between
+ * (the step sequence is captured once in a CUDA graph and replayed). */
+int wx3d_run(wx_ctx* ctx, int32_t nsteps, wx_state* out);
+/* Same, enqueued on the context stream without a final synchronisation. */
+int wx3d_run_async(wx_ctx* ctx, int32_t nsteps);
+
+/* loadcooldata (source/cooling.f90:135-184): npts rows (logT, b) with the
+ * cooling rate stored as -b (cooltable(2,i) = -b). */
+int wx3d_set_cooltable(wx_ctx* ctx, int32_t npts, const double* logT, const double* b);
+
+/* markByPhysical (source/amr.f90:142-230) for every occupied slot:
+ * flags[slot] = WX_FLAG_*; empty slots get -1. */
+int wx3d_mark(wx_ctx* ctx, int32_t nslots, int32_t* flags);
+
+/* Data part of refineBlock (source/amr.f90:355-367): injection of the
+ * father's octants into 8 child slots (children in x,y,z natural order). */
+int wx3d_refine(wx_ctx* ctx, int32_t father_slot, const int32_t* child_slots8);
+
+/* Data part of coarseBlocks (source/amr.f90:1597-1625): 8-cell averages of
+ * the 8 siblings (natural order) into the father slot. */
+int wx3d_coarsen(wx_ctx* ctx, const int32_t* child_slots8, int32_t father_slot);
+
+/* Per-kernel device timing with CUDA events recorded around each launch of
+ * the step sequence (inside the CUDA graph of wx3d_run).  wx3d_kernel_times
+ * returns, for the last step(s) executed, the summed milliseconds and the
+ * launch counts of: [0] predictor stage, [1] corrector (or single) stage,
+ * [2] viscous step + CFL reduction, [3] source terms. */
+int wx3d_set_timing(wx_ctx* ctx, int32_t on);
+int wx3d_kernel_times(wx_ctx* ctx, double* ms4, int32_t* count4);
+
+int wx3d_get_status(wx_ctx* ctx, wx_status* st);
+int wx3d_reset_status(wx_ctx* ctx);
+
+/* Human-readable text of a status code and of the context's last error. */
+const char* wx3d_error_string(int32_t code);
+int wx3d_last_error(wx_ctx* ctx, char* buf, int32_t len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WX3D_H */

@@ -1,0 +1,117 @@
+"""Physics pins of the CPU oracle (the reference ships no golden data):
+exact Riemann solutions, FP64 conservation, symmetry, Brio-Wu structure."""
+import numpy as np
+import pytest
+
+import oracle
+from walicxe3d_b200 import config as C
+from walicxe3d_b200 import problems
+
+from exact_riemann import sample
+
+
+def run_to(o, t_end, max_steps=5000):
+    n = 0
+    while o.state.time < t_end - 1e-15 and n < max_steps:
+        o.step()
+        n += 1
+    return n
+
+
+def profile(prob, arr, axis):
+    """1-D profile along `axis` of a [nb, ...] array on a single-level tube."""
+    order = np.argsort([prob.tree.coords(int(b))[1][axis] for b in prob.local_blocks])
+    out = []
+    for n in order:
+        a = arr[n]
+        ax = {0: 2, 1: 1, 2: 0}[axis]
+        other = tuple(d for d in range(3) if d != ax)
+        line = a.mean(axis=other)
+        spread = np.ptp(a, axis=other).max()
+        assert spread < 1e-12, "tube solution is not uniform across the tube"
+        out.append(line)
+    return np.concatenate(out)
+
+
+@pytest.mark.parametrize("solver,limiter,axis,tol", [
+    (C.SOLVER_HLLC, C.LIMITER_MINMOD, 0, 0.006),
+    (C.SOLVER_HLLC, C.LIMITER_VANLEER, 1, 0.005),
+    (C.SOLVER_HLL, C.LIMITER_MINMOD, 2, 0.008),
+    (C.SOLVER_HLL1, C.LIMITER_MINMOD, 0, 0.02),
+    (C.SOLVER_LAX, C.LIMITER_MINMOD, 0, 0.06),
+])
+def test_sod_exact(solver, limiter, axis, tol, ncpu):
+    prob = problems.shock_tube(nblocks=8, axis=axis, solver=solver, limiter=limiter, eta=0.0, t_end=0.15)
+    o = oracle.from_problem(prob, threads=ncpu)
+    run_to(o, 0.15)
+    assert abs(o.state.time - 0.15) < 1e-14
+    rho = profile(prob, o.U[:, 0], axis)
+    n = len(rho)
+    x = (np.arange(n) + 0.5) / n
+    ex = sample(x, 0.15, 0.5, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1, 1.4)
+    l1 = np.abs(rho - ex[0]).mean()
+    assert l1 < tol, f"L1(rho) = {l1}"
+
+
+def test_sedov_conservation_and_symmetry(ncpu):
+    prob = problems.sedov(4)
+    prob.cfg.visc_eta = 0.0
+    o = oracle.from_problem(prob, threads=ncpu)
+    U0 = o.U
+    for _ in range(30):
+        o.step()
+    U = o.U
+    for e in (0, 4):
+        assert abs(U[:, e].sum() - U0[:, e].sum()) <= 1e-13 * abs(U0[:, e].sum())
+    G = np.zeros((64, 64, 64))
+    for n, b in enumerate(prob.local_blocks):
+        _, x = prob.tree.coords(int(b))
+        G[x[2] * 16:(x[2] + 1) * 16, x[1] * 16:(x[1] + 1) * 16, x[0] * 16:(x[0] + 1) * 16] = U[n, 0]
+    assert np.abs(G - G[:, :, ::-1]).max() < 1e-12
+    assert np.abs(G - G.transpose(0, 2, 1)).max() < 1e-12
+    assert np.abs(G - G.transpose(2, 1, 0)).max() < 1e-12
+
+
+def test_viscosity_breaks_exact_conservation_at_block_faces(ncpu):
+    """doViscousStep takes face neighbours from the half-step ghosts
+    (hydro_solver.f90:217-250 after godunov.f90:141), so with eta>0 the
+    mass changes by more than round-off; with a single block it does not."""
+    prob = problems.sedov(2)
+    o = oracle.from_problem(prob, threads=ncpu)
+    m0 = o.U[:, 0].sum()
+    for _ in range(20):
+        o.step()
+    assert abs(o.U[:, 0].sum() - m0) > 1e-12 * m0
+
+
+def test_brio_wu_structure(ncpu):
+    prob = problems.brio_wu(16)
+    o = oracle.from_problem(prob, threads=ncpu)
+    m0 = o.U[:, 0].sum()
+    run_to(o, 0.1)
+    U = o.U
+    rho = profile(prob, U[:, 0], 0)
+    by = profile(prob, U[:, 6], 0)
+    assert abs(U[:, 0].sum() - m0) <= 1e-12 * m0     # waves stay inside the box
+    assert rho.min() > 0.1 and rho.max() < 1.0 + 1e-9
+    assert by[0] == pytest.approx(1.0) and by[-1] == pytest.approx(-1.0)
+    # compound wave and slow shock: density between the two plateaus
+    mid = rho[(np.arange(256) > 120) & (np.arange(256) < 150)]
+    assert mid.min() < 0.75 and mid.max() > 0.5
+    assert np.all(np.isfinite(U))
+
+
+def test_dt_ramp_and_clip(ncpu):
+    """getTimestep: 2^-(11-it) ramp for it<=10 (hydro_solver.f90:191-194)
+    and clipping to the next output time (:204-207)."""
+    prob = problems.sedov(2)
+    o = oracle.from_problem(prob, threads=ncpu)
+    o.set_state(0.0, 0.0, 1, 1, 0)
+    d1 = o.get_timestep()
+    o.set_state(0.0, 0.0, 11, 1, 0)
+    d11 = o.get_timestep()
+    assert d1 == pytest.approx(d11 / 1024.0, rel=1e-15)
+    prob2 = problems.shock_tube(nblocks=2, t_end=1e-6)
+    o2 = oracle.from_problem(prob2, threads=ncpu)
+    o2.set_state(0.0, 0.0, 11, 1, 0)
+    assert o2.get_timestep() == 1e-6

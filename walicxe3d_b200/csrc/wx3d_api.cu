@@ -1,0 +1,917 @@
+// wx3d_api.cu -- C-ABI of the B200 per-block Godunov update (include/wx3d.h).
+//
+// Host side: context, neighbour-table construction from the localBlocks
+// registry (restating the bID arithmetic of source/amr.f90:439-1098),
+// uploads and downloads, and the step sequence of source/main.f90:81-100
+// enqueued on one CUDA stream (replayed from a CUDA graph by wx3d_run).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/wx3d.h"
+#include "wx3d_kernels.cuh"
+#include "wx3d_source.cuh"
+
+using namespace wx;
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Kernel table per (neq, mhd, solver)
+
+struct Kern {
+  void (*stage1)(StageParams) = nullptr;
+  void (*stage2)(StageParams) = nullptr;
+  void (*lax)(LaxParams) = nullptr;
+  void (*visc)(ViscParams) = nullptr;
+  void (*dt)(DtParams) = nullptr;
+  void (*src)(SrcParams) = nullptr;
+  void (*mark)(MarkParams) = nullptr;
+  void (*prims)(const double*, double*, const int32_t*, int, DevCtl*, double) = nullptr;
+  size_t smem = 0;
+};
+
+template <int NEQ, bool MHD, int SOLVER>
+Kern make_kern() {
+  Kern k;
+  k.stage1 = stage_kernel<NEQ, MHD, SOLVER, 1>;
+  k.stage2 = stage_kernel<NEQ, MHD, SOLVER, 2>;
+  k.lax = lax_kernel<NEQ, MHD>;
+  k.visc = viscous_kernel<NEQ, MHD>;
+  k.dt = dt_kernel<NEQ, MHD>;
+  k.src = source_kernel<NEQ, MHD>;
+  k.mark = mark_kernel<NEQ, MHD>;
+  k.prims = prims_kernel<NEQ, MHD>;
+  k.smem = stage_smem_bytes<NEQ>();
+  return k;
+}
+
+// Supported combinations: hydro with 0..2 passives (HLL/HLL1/HLLC/LAX) and
+// ideal MHD without passives (HLL/HLL1/HLLE/HLLD/LAX).
+bool select_kern(const wx_config& c, Kern& k) {
+  const bool mhd = c.bfield != 0;
+  const int s = c.solver_type;
+  const int rs = (s == WX_SOLVER_HLL1 || s == WX_SOLVER_LAX) ? WX_SOLVER_HLL : s;
+  if (!mhd) {
+    if (rs != WX_SOLVER_HLL && rs != WX_SOLVER_HLLC) return false;
+    const bool c_ = rs == WX_SOLVER_HLLC;
+    switch (c.neqtot) {
+      case 5: k = c_ ? make_kern<5, false, WX_SOLVER_HLLC>() : make_kern<5, false, WX_SOLVER_HLL>(); return true;
+      case 6: k = c_ ? make_kern<6, false, WX_SOLVER_HLLC>() : make_kern<6, false, WX_SOLVER_HLL>(); return true;
+      case 7: k = c_ ? make_kern<7, false, WX_SOLVER_HLLC>() : make_kern<7, false, WX_SOLVER_HLL>(); return true;
+      default: return false;
+    }
+  }
+  if (c.neqtot != 8) return false;
+  switch (rs) {
+    case WX_SOLVER_HLL: k = make_kern<8, true, WX_SOLVER_HLL>(); return true;
+    case WX_SOLVER_HLLE: k = make_kern<8, true, WX_SOLVER_HLLE>(); return true;
+    case WX_SOLVER_HLLD: k = make_kern<8, true, WX_SOLVER_HLLD>(); return true;
+    default: return false;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Block tree arithmetic (source/amr.f90), independent of the process layout.
+
+struct Tree {
+  int nbroot[3] = {1, 1, 1};
+  int maxlev = 1;
+  int nb[WX3D_MAX_LEVELS + 2][3] = {};
+  long long minID[WX3D_MAX_LEVELS + 2] = {}, maxID[WX3D_MAX_LEVELS + 2] = {};
+
+  void init(const wx_config& c) {  // init.f90:733-756
+    nbroot[0] = c.nbrootx; nbroot[1] = c.nbrooty; nbroot[2] = c.nbrootz;
+    maxlev = c.maxlev;
+    long long acc = 0;
+    for (int l = 1; l <= maxlev; ++l) {
+      for (int d = 0; d < 3; ++d) nb[l][d] = nbroot[d] << (l - 1);
+      long long n = (long long)nb[l][0] * nb[l][1] * nb[l][2];
+      minID[l] = acc + 1;
+      maxID[l] = acc + n;
+      acc += n;
+    }
+  }
+  int level(long long bID) const {  // meshlevel, amr.f90:637
+    for (int l = 1; l <= maxlev; ++l) if (bID >= minID[l] && bID <= maxID[l]) return l;
+    return -1;
+  }
+  void coords(long long bID, int l, int x[3]) const {  // bcoords, amr.f90:972 (0-based here)
+    long long loc = bID - minID[l];
+    x[0] = (int)(loc % nb[l][0]);
+    x[1] = (int)((loc / nb[l][0]) % nb[l][1]);
+    x[2] = (int)(loc / ((long long)nb[l][0] * nb[l][1]));
+  }
+  long long id(int l, const int x[3]) const {
+    return minID[l] + x[0] + (long long)nb[l][0] * (x[1] + (long long)nb[l][1] * x[2]);
+  }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+
+struct wx_ctx {
+  wx_config cfg{};
+  PhysParams ph{};
+  Kern k;
+  int neq = 5;
+  int max_blocks = 0;
+  int dev = 0, nsm = 148;
+  cudaStream_t own = nullptr, stream = nullptr;
+  double* dU = nullptr;
+  double* dUP = nullptr;
+  double* dW = nullptr;
+  double* dPrim = nullptr;
+  double* dStage = nullptr;  // staging slab for the Fortran layout
+  size_t stage_bytes = 0;
+  DevBlock* dBlocks = nullptr;
+  int32_t* dWork = nullptr;
+  int32_t* dFlags = nullptr;
+  DevCtl* dCtl = nullptr;
+  DevCtl* hCtl = nullptr;   // pinned mirror
+  double* dCool = nullptr;  // [2][ncool]
+  int ncool = 0;
+  Tree tree;
+  std::vector<int32_t> local;     // localBlocks
+  std::vector<int32_t> work;      // occupied slots
+  std::vector<DevBlock> hblocks;
+  int nwork = 0;
+  int zsplit = 1;
+  int grid_stage = 0, grid_256 = 0;
+  bool dt_valid = false;
+  bool prestep = false;           // dW holds the state at the start of the last step
+  cudaGraphExec_t graph = nullptr;
+  bool graph_valid = false;
+  long long launches = 0;
+  // per-kernel timing: event pairs around the launches of one step sequence
+  bool timing = false;
+  bool timing_mute = false;
+  cudaEvent_t ev[64] = {};
+  int ev_kind[32] = {};
+  int nev = 0;
+  std::string err;
+};
+
+namespace {
+
+int fail(wx_ctx* c, int code, const char* fmt, ...) {
+  if (c) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    c->err = buf;
+  }
+  return code;
+}
+
+#define WX_CUDA(call)                                                                           \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess) return fail(c, WX_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+#define WX_LAUNCHED()                                                                     \
+  do {                                                                                    \
+    cudaError_t e_ = cudaGetLastError();                                                  \
+    if (e_ != cudaSuccess) return fail(c, WX_ERR_CUDA, "launch: %s", cudaGetErrorString(e_)); \
+    ++c->launches;                                                                        \
+  } while (0)
+
+int validate(const wx_config& f, std::string& why) {
+  if (f.neqtot != 5 + 3 * (f.bfield ? 1 : 0) + f.npassive) { why = "neqtot != 5 + 3*bfield + npassive"; return WX_ERR_INVALID_ARG; }
+  if (f.neqtot > WX3D_MAX_NEQ) { why = "neqtot too large"; return WX_ERR_INVALID_ARG; }
+  if (f.maxlev < 1 || f.maxlev > WX3D_MAX_LEVELS) { why = "maxlev out of 1..10"; return WX_ERR_TOO_MANY_LEVS; }
+  if (f.nbrootx < 1 || f.nbrooty < 1 || f.nbrootz < 1) { why = "root block counts must be >= 1"; return WX_ERR_INVALID_ARG; }
+  if (f.mhd && !f.bfield) { why = "mhd without bfield computes no time step in the reference"; return WX_ERR_UNSUPPORTED; }
+  if (f.bfield && !f.mhd) { why = "passive magnetic field (bfield without mhd) is not supported"; return WX_ERR_UNSUPPORTED; }
+  if (f.user_source_terms) { why = "user source terms are not part of this ABI"; return WX_ERR_UNSUPPORTED; }
+  for (int i = 0; i < 6; ++i) {
+    if (f.bc[i] == WX_BC_PERIODIC) { why = "BC_PERIODIC is not implemented by the reference (ghosts stay stale)"; return WX_ERR_UNSUPPORTED; }
+    if (f.bc[i] != WX_BC_REFLECTIVE && f.bc[i] != WX_BC_FREE_FLOW) { why = "unknown boundary condition"; return WX_ERR_INVALID_ARG; }
+  }
+  if ((f.eos_type == WX_EOS_H_RATE || f.cooling_type == WX_COOL_H) && f.npassive < 1) { why = "H-rate EOS / COOL_H need a passive scalar"; return WX_ERR_NOT_ENOUGH_PASSIVES; }
+  if (f.cooling_type == WX_COOL_TABLE_METAL || f.cooling_type == WX_COOL_SCHURE) { why = "cooling type not supported by this ABI"; return WX_ERR_UNSUPPORTED; }
+  if (f.gamma <= 1.0) { why = "gamma must exceed 1"; return WX_ERR_INVALID_ARG; }
+  return WX_OK;
+}
+
+void fill_phys(wx_ctx* c) {
+  const wx_config& f = c->cfg;
+  PhysParams& p = c->ph;
+  p.gamma = f.gamma;
+  p.cv = 1.0 / (f.gamma - 1.0);           // parameters.f90:373
+  p.cfl = f.cfl;
+  p.eta = f.visc_eta;
+  p.mu0 = f.mu0; p.mui = f.mui; p.ion_thres = f.ion_thres;
+  p.d_sc = f.d_sc;
+  p.p_sc = f.d_sc * (f.v_sc * f.v_sc);    // parameters.f90:379
+  p.e_sc = p.p_sc;                        // :380
+  p.t_sc = f.l_sc / f.v_sc;               // :381
+  p.dtout = f.dtout;
+  p.cooling_limit = f.cooling_limit;
+  p.limiter = f.limiter_type;
+  p.eight_wave = f.eight_wave;
+  for (int i = 0; i < 6; ++i) p.bc[i] = f.bc[i];
+  p.eos = f.eos_type;
+  p.cooling = f.cooling_type;
+  p.fp = 5 + 3 * (f.bfield ? 1 : 0);
+  p.npassive = f.npassive;
+}
+
+bool sources_on(const wx_ctx* c) { return c->cfg.eos_type == WX_EOS_H_RATE || c->cfg.cooling_type != WX_COOL_NONE; }
+
+// kinds: 0 stage1, 1 stage2 (or the single stage), 2 viscous, 3 sources
+void tick(wx_ctx* c, int kind, bool begin) {
+  if (!c->timing || c->timing_mute || c->nev >= 64) return;
+  if (begin) c->ev_kind[c->nev / 2] = kind;
+  cudaEventRecord(c->ev[c->nev], c->stream);
+  ++c->nev;
+}
+
+int grid_for(wx_ctx* c, const void* fn, int threads, size_t smem, int items) {
+  int per = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, smem);
+  per = std::max(per, 1);
+  return std::max(1, std::min(items, per * c->nsm));
+}
+
+int set_stage_attrs(wx_ctx* c) {
+  WX_CUDA(cudaFuncSetAttribute(c->k.stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->k.smem));
+  WX_CUDA(cudaFuncSetAttribute(c->k.stage2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->k.smem));
+  return WX_OK;
+}
+
+// ---- step pieces -------------------------------------------------------------
+
+int launch_dt(wx_ctx* c, const double* u) {
+  ctl_reset_dtmin_kernel<<<1, 1, 0, c->stream>>>(c->dCtl);
+  WX_LAUNCHED();
+  DtParams P{u, c->dBlocks, c->dWork, c->nwork, c->dCtl, c->ph};
+  c->k.dt<<<grid_for(c, (const void*)c->k.dt, 256, 0, c->nwork), 256, 0, c->stream>>>(P);
+  WX_LAUNCHED();
+  return WX_OK;
+}
+
+int launch_stage(wx_ctx* c, int order, const double* src, const double* base, double* out, double factor) {
+  StageParams P{src, base, out, c->dBlocks, c->dWork, c->nwork * c->zsplit, c->zsplit, c->dCtl, factor, c->ph};
+  auto fn = order == 1 ? c->k.stage1 : c->k.stage2;
+  const int grid = grid_for(c, (const void*)fn, STAGE_THREADS, c->k.smem, c->nwork * c->zsplit);
+  const int kind = (order == 2 || factor == 1.0) ? 1 : 0;
+  tick(c, kind, true);
+  fn<<<grid, STAGE_THREADS, c->k.smem, c->stream>>>(P);
+  WX_LAUNCHED();
+  tick(c, kind, false);
+  return WX_OK;
+}
+
+// Godunov(order)/LaxFriedrichs + doViscousStep; on return dU holds U^{n+1}.
+int enqueue_solver(wx_ctx* c, bool bump_it, bool finish_output) {
+  const int solver = c->cfg.solver_type;
+  const bool src = sources_on(c);
+  step_begin_kernel<<<1, 1, 0, c->stream>>>(c->dCtl, c->ph.cfl, c->cfg.cooling_type != WX_COOL_NONE, c->ph.dtout,
+                                            c->ph.t_sc, bump_it ? 1 : 0);
+  WX_LAUNCHED();
+  int zero_ghost = 0;
+  int rc;
+  if (solver == WX_SOLVER_LAX) {
+    LaxParams P{c->dU, c->dW, c->dBlocks, c->dWork, c->nwork, c->dCtl, c->ph};
+    tick(c, 1, true);
+    c->k.lax<<<grid_for(c, (const void*)c->k.lax, 256, 0, c->nwork), 256, 0, c->stream>>>(P);
+    WX_LAUNCHED();
+    tick(c, 1, false);
+    zero_ghost = 1;
+  } else if (solver == WX_SOLVER_HLL1) {
+    if ((rc = launch_stage(c, 1, c->dU, c->dU, c->dW, 1.0))) return rc;
+    zero_ghost = 1;
+  } else {
+    if ((rc = launch_stage(c, 1, c->dU, c->dU, c->dUP, 0.5))) return rc;
+    if ((rc = launch_stage(c, 2, c->dUP, c->dU, c->dW, 1.0))) return rc;
+  }
+  ViscParams V{c->dW, c->dUP, c->dBlocks, c->dWork, c->nwork, zero_ghost, src ? 0 : 1, c->dCtl, c->ph};
+  tick(c, 2, true);
+  c->k.visc<<<grid_for(c, (const void*)c->k.visc, 256, 0, c->nwork), 256, 0, c->stream>>>(V);
+  WX_LAUNCHED();
+  tick(c, 2, false);
+  step_end_kernel<<<1, 1, 0, c->stream>>>(c->dCtl, finish_output ? 1 : 0);
+  WX_LAUNCHED();
+  std::swap(c->dU, c->dW);
+  c->prestep = true;
+  c->dt_valid = !src;
+  return WX_OK;
+}
+
+// mode bits: 1 = hrate, 2 = cooling, 4 = read/write the PRIM buffer, 8 = CFL minimum
+int enqueue_sources(wx_ctx* c, int mode) {
+  if (mode & 8) {
+    ctl_reset_dtmin_kernel<<<1, 1, 0, c->stream>>>(c->dCtl);
+    WX_LAUNCHED();
+  }
+  SrcParams P{c->dU, (mode & 4) ? c->dPrim : nullptr, c->dBlocks, c->dWork, c->nwork, mode, c->dCtl,
+              c->dCool, c->dCool ? c->dCool + c->ncool : nullptr, c->ncool, c->ph};
+  tick(c, 3, true);
+  c->k.src<<<grid_for(c, (const void*)c->k.src, 256, 0, c->nwork), 256, 0, c->stream>>>(P);
+  WX_LAUNCHED();
+  tick(c, 3, false);
+  if (mode & 8) c->dt_valid = true;
+  return WX_OK;
+}
+
+int enqueue_step(wx_ctx* c) {
+  int rc;
+  if (!c->dt_valid) {
+    if ((rc = launch_dt(c, c->dU))) return rc;
+    c->dt_valid = true;
+  }
+  if ((rc = enqueue_solver(c, true, true))) return rc;
+  if (sources_on(c)) {
+    int mode = 8;
+    if (c->cfg.eos_type == WX_EOS_H_RATE) mode |= 1;
+    if (c->cfg.cooling_type != WX_COOL_NONE) mode |= 2;
+    if ((rc = enqueue_sources(c, mode))) return rc;
+  }
+  return WX_OK;
+}
+
+int sync_check(wx_ctx* c) {
+  WX_CUDA(cudaMemcpyAsync(c->hCtl, c->dCtl, sizeof(DevCtl), cudaMemcpyDeviceToHost, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->hCtl->cnt[2]) return fail(c, WX_ERR_DIVISION_BY_ZERO, "zero density in flow2prim (%llu cells)", c->hCtl->cnt[2]);
+  if (c->hCtl->cnt[3]) return fail(c, WX_ERR_NAN, "non-finite state after the step (%llu values)", c->hCtl->cnt[3]);
+  return WX_OK;
+}
+
+void invalidate_graph(wx_ctx* c) {
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  c->graph = nullptr;
+  c->graph_valid = false;
+}
+
+bool ready(wx_ctx* c) { return c && c->nwork > 0; }
+
+}  // namespace
+
+// =============================================================================
+extern "C" {
+
+int wx3d_config_defaults(wx_config* f) {
+  if (!f) return WX_ERR_INVALID_ARG;
+  std::memset(f, 0, sizeof *f);
+  f->neqtot = 5;
+  f->solver_type = WX_SOLVER_HLLC;
+  f->limiter_type = WX_LIMITER_VANLEER;
+  f->eos_type = WX_EOS_ADIABATIC;
+  f->cooling_type = WX_COOL_NONE;
+  for (int i = 0; i < 6; ++i) f->bc[i] = WX_BC_FREE_FLOW;
+  f->nbrootx = f->nbrooty = f->nbrootz = 1;
+  f->maxlev = 1;
+  f->gamma = 5.0 / 3.0;
+  f->cfl = 0.4;
+  f->visc_eta = 5.0e-3;
+  f->cooling_limit = 0.5;
+  f->mu0 = 1.3; f->mui = 0.61; f->ion_thres = 1.0e4;
+  f->l_sc = f->d_sc = f->v_sc = 1.0;
+  f->xphystot = f->yphystot = f->zphystot = 1.0;
+  f->tfin = 1.0e30; f->dtout = 1.0e30;
+  f->refine_thres = 0.3; f->coarse_thres = 0.03;
+  return WX_OK;
+}
+
+const char* wx3d_error_string(int32_t code) {
+  switch (code) {
+    case WX_OK: return "ok";
+    case WX_ERR_INSUFICIENT_NBMAXPROC: return "not enough block slots";
+    case WX_ERR_TOO_MANY_LEVS: return "too many refinement levels";
+    case WX_ERR_COOLING_LOAD_COEFS: return "bad cooling table";
+    case WX_ERR_DIVISION_BY_ZERO: return "zero density";
+    case WX_ERR_NOT_ENOUGH_PASSIVES: return "not enough passive scalars";
+    case WX_ERR_NAN_IN_FLUXES: return "NaN in fluxes";
+    case WX_ERR_CUDA: return "CUDA error";
+    case WX_ERR_TIMEOUT: return "device wait timed out";
+    case WX_ERR_NAN: return "non-finite state";
+    case WX_ERR_INVALID_ARG: return "invalid argument";
+    case WX_ERR_UNSUPPORTED: return "unsupported configuration";
+    case WX_ERR_NO_DEVICE: return "no CUDA device";
+    case WX_ERR_MESH: return "invalid mesh";
+    default: return "generic error";
+  }
+}
+
+int wx3d_last_error(wx_ctx* c, char* buf, int32_t len) {
+  if (!c || !buf || len <= 0) return WX_ERR_INVALID_ARG;
+  std::snprintf(buf, (size_t)len, "%s", c->err.c_str());
+  return WX_OK;
+}
+
+int wx3d_init(const wx_config* cfg, int32_t max_blocks, wx_ctx** out) {
+  if (!cfg || !out || max_blocks <= 0) return WX_ERR_INVALID_ARG;
+  *out = nullptr;
+  std::string why;
+  int rc = validate(*cfg, why);
+  if (rc) { std::fprintf(stderr, "wx3d_init: %s\n", why.c_str()); return rc; }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return WX_ERR_NO_DEVICE;
+  wx_ctx* c = new wx_ctx();
+  c->cfg = *cfg;
+  c->neq = cfg->neqtot;
+  c->max_blocks = max_blocks;
+  if (!select_kern(*cfg, c->k)) { delete c; std::fprintf(stderr, "wx3d_init: solver/equation set not supported\n"); return WX_ERR_UNSUPPORTED; }
+  fill_phys(c);
+  c->tree.init(*cfg);
+  cudaGetDevice(&c->dev);
+  cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev);
+  auto cleanup = [&](int code) { wx3d_finalize(c); return code; };
+  if ((rc = set_stage_attrs(c))) return cleanup(rc);
+  const size_t n = (size_t)max_blocks * c->neq * BCELLS;
+  if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) return cleanup(WX_ERR_CUDA);
+  c->stream = c->own;
+  if (cudaMalloc(&c->dU, n * 8) || cudaMalloc(&c->dUP, n * 8) || cudaMalloc(&c->dW, n * 8)) return cleanup(WX_ERR_CUDA);
+  cudaMemset(c->dU, 0, n * 8);
+  cudaMemset(c->dUP, 0, n * 8);
+  cudaMemset(c->dW, 0, n * 8);
+  if (cudaMalloc(&c->dBlocks, sizeof(DevBlock) * max_blocks) || cudaMalloc(&c->dWork, 4 * (size_t)max_blocks) ||
+      cudaMalloc(&c->dFlags, 4 * (size_t)max_blocks) || cudaMalloc(&c->dCtl, sizeof(DevCtl)) ||
+      cudaMallocHost(&c->hCtl, sizeof(DevCtl)))
+    return cleanup(WX_ERR_CUDA);
+  std::memset(c->hCtl, 0, sizeof(DevCtl));
+  c->hCtl->nextout = 1;
+  {
+    const double big = 1.0e30;
+    std::memcpy(&c->hCtl->dtmin_bits, &big, 8);
+  }
+  if (cudaMemcpy(c->dCtl, c->hCtl, sizeof(DevCtl), cudaMemcpyHostToDevice)) return cleanup(WX_ERR_CUDA);
+  c->local.assign(max_blocks, -1);
+  c->hblocks.assign(max_blocks, DevBlock{});
+  *out = c;
+  return WX_OK;
+}
+
+int wx3d_finalize(wx_ctx* c) {
+  if (!c) return WX_ERR_INVALID_ARG;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  invalidate_graph(c);
+  cudaFree(c->dU); cudaFree(c->dUP); cudaFree(c->dW); cudaFree(c->dPrim); cudaFree(c->dStage);
+  cudaFree(c->dBlocks); cudaFree(c->dWork); cudaFree(c->dFlags); cudaFree(c->dCtl); cudaFree(c->dCool);
+  if (c->hCtl) cudaFreeHost(c->hCtl);
+  for (int i = 0; i < 64; ++i)
+    if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+  return WX_OK;
+}
+
+int wx3d_set_stream(wx_ctx* c, void* s) {
+  if (!c) return WX_ERR_INVALID_ARG;
+  cudaStreamSynchronize(c->stream);
+  c->stream = s ? (cudaStream_t)s : c->own;
+  invalidate_graph(c);
+  return WX_OK;
+}
+
+// Neighbour table from the localBlocks registry (amr.f90:539-631 neighbors,
+// :831 siblingCoords, :916 father, :882 children).
+int wx3d_set_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb) {
+  if (!c || !lb || nslots < 0) return WX_ERR_INVALID_ARG;
+  if (nslots > c->max_blocks) return fail(c, WX_ERR_INSUFICIENT_NBMAXPROC, "%d slots > max_blocks %d", nslots, c->max_blocks);
+  const Tree& T = c->tree;
+  std::unordered_map<long long, int> slot;
+  slot.reserve((size_t)nslots * 2);
+  for (int s = 0; s < nslots; ++s) {
+    if (lb[s] == -1) continue;
+    if (T.level(lb[s]) < 1) return fail(c, WX_ERR_MESH, "slot %d: bID %d outside the tree", s, lb[s]);
+    if (!slot.emplace(lb[s], s).second) return fail(c, WX_ERR_MESH, "bID %d registered twice", lb[s]);
+  }
+  std::vector<DevBlock> hb(c->max_blocks);
+  std::vector<int32_t> work;
+  for (int s = 0; s < nslots; ++s) {
+    DevBlock b{};
+    const long long id = lb[s];
+    if (id == -1) { hb[s] = b; continue; }
+    const int l = T.level(id);
+    int x[3];
+    T.coords(id, l, x);
+    b.level = l;
+    b.bID = (int32_t)id;
+    for (int d = 0; d < 3; ++d) {
+      b.bc[d] = x[d] + 1;
+      b.sib[d] = l > 1 ? (x[d] & 1) : -1;
+    }
+    const double s2 = std::ldexp(1.0, l - 1);
+    b.dx = c->cfg.xphystot / ((double)(NC * c->cfg.nbrootx) * s2) / c->cfg.l_sc;
+    b.dy = c->cfg.yphystot / ((double)(NC * c->cfg.nbrooty) * s2) / c->cfg.l_sc;
+    b.dz = c->cfg.zphystot / ((double)(NC * c->cfg.nbrootz) * s2) / c->cfg.l_sc;
+    for (int f = 0; f < 6; ++f) {
+      const int ax = f / 2, side = f & 1;
+      for (int q = 0; q < 4; ++q) b.fnb[f][q] = -1;
+      int y[3] = {x[0], x[1], x[2]};
+      y[ax] += side ? 1 : -1;
+      if (y[ax] < 0 || y[ax] >= T.nb[l][ax]) { b.ftype[f] = WX_NEIGH_BOUNDARY; continue; }
+      const long long nID = T.id(l, y);
+      auto it = slot.find(nID);
+      if (it != slot.end()) { b.ftype[f] = WX_NEIGH_SAME; b.fnb[f][0] = it->second; continue; }
+      if (l > 1) {
+        int z[3] = {y[0] / 2, y[1] / 2, y[2] / 2};
+        auto ft = slot.find(T.id(l - 1, z));
+        if (ft != slot.end()) { b.ftype[f] = WX_NEIGH_COARSER; b.fnb[f][0] = ft->second; continue; }
+      }
+      // finer: the four children of nID adjacent to this face, transverse
+      // axes in x<y<z order (amr.f90:590-628)
+      if (l >= T.maxlev) return fail(c, WX_ERR_MESH, "bID %lld face %d: no active neighbour", id, f + 1);
+      const int t1 = ax == 0 ? 1 : 0, t2 = ax == 2 ? 1 : 2;
+      b.ftype[f] = WX_NEIGH_FINER;
+      for (int q = 0; q < 4; ++q) {
+        int ch[3];
+        ch[ax] = 2 * y[ax] + (side ? 0 : 1);
+        ch[t1] = 2 * y[t1] + (q & 1);
+        ch[t2] = 2 * y[t2] + (q >> 1);
+        auto ct = slot.find(T.id(l + 1, ch));
+        if (ct == slot.end())
+          return fail(c, WX_ERR_MESH, "bID %lld face %d: neighbour region is neither same, coarser nor finer by one", id, f + 1);
+        b.fnb[f][q] = ct->second;
+      }
+    }
+    hb[s] = b;
+    work.push_back(s);
+  }
+  c->local.assign(c->max_blocks, -1);
+  std::copy(lb, lb + nslots, c->local.begin());
+  c->hblocks = hb;
+  c->work = work;
+  c->nwork = (int)work.size();
+  WX_CUDA(cudaMemcpyAsync(c->dBlocks, hb.data(), sizeof(DevBlock) * c->max_blocks, cudaMemcpyHostToDevice, c->stream));
+  if (!work.empty())
+    WX_CUDA(cudaMemcpyAsync(c->dWork, work.data(), 4 * work.size(), cudaMemcpyHostToDevice, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  // small meshes split every block into z-slabs so all SMs get work
+  c->zsplit = 1;
+  while (c->zsplit < 8 && c->nwork * c->zsplit < 2 * c->nsm) c->zsplit *= 2;
+  c->dt_valid = false;
+  c->prestep = false;
+  invalidate_graph(c);
+  return WX_OK;
+}
+
+int wx3d_set_zsplit(wx_ctx* c, int32_t zsplit) {
+  if (!c || (zsplit != 1 && zsplit != 2 && zsplit != 4 && zsplit != 8)) return WX_ERR_INVALID_ARG;
+  c->zsplit = zsplit;
+  invalidate_graph(c);
+  return WX_OK;
+}
+
+int wx3d_get_neighbours(wx_ctx* c, int32_t nslots, int32_t* ft, int32_t* fs) {
+  if (!c || !ft || !fs || nslots > c->max_blocks) return WX_ERR_INVALID_ARG;
+  for (int s = 0; s < nslots; ++s)
+    for (int f = 0; f < 6; ++f) {
+      ft[s * 6 + f] = c->hblocks[s].ftype[f];
+      for (int q = 0; q < 4; ++q) fs[(s * 6 + f) * 4 + q] = c->hblocks[s].fnb[f][q];
+    }
+  return WX_OK;
+}
+
+int wx3d_upload_blocks(wx_ctx* c, int32_t nslots, const double* u) {
+  if (!c || !u || nslots < 0 || nslots > c->max_blocks) return WX_ERR_INVALID_ARG;
+  WX_CUDA(cudaMemcpyAsync(c->dU, u, (size_t)nslots * c->neq * BCELLS * 8, cudaMemcpyHostToDevice, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  c->dt_valid = false;
+  c->prestep = false;
+  return WX_OK;
+}
+
+int wx3d_download_blocks(wx_ctx* c, int32_t nslots, double* u) {
+  if (!c || !u || nslots < 0 || nslots > c->max_blocks) return WX_ERR_INVALID_ARG;
+  WX_CUDA(cudaMemcpyAsync(u, c->dU, (size_t)nslots * c->neq * BCELLS * 8, cudaMemcpyDeviceToHost, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  return WX_OK;
+}
+
+static int ensure_stage(wx_ctx* c, size_t bytes) {
+  if (c->stage_bytes >= bytes) return WX_OK;
+  cudaFree(c->dStage);
+  c->dStage = nullptr;
+  c->stage_bytes = 0;
+  WX_CUDA(cudaMalloc(&c->dStage, bytes));
+  c->stage_bytes = bytes;
+  return WX_OK;
+}
+
+int wx3d_upload_U_fortran(wx_ctx* c, int32_t nbmax, const double* U) {
+  if (!c || !U || nbmax <= 0) return WX_ERR_INVALID_ARG;
+  const int ns = std::min(nbmax, c->max_blocks);
+  const size_t slab = (size_t)nbmax * c->neq * 400;  // U(:,:,:,:,k) for one k
+  int rc;
+  if ((rc = ensure_stage(c, slab * 8))) return rc;
+  for (int kf = 1; kf <= NC; ++kf) {
+    WX_CUDA(cudaMemcpyAsync(c->dStage, U + slab * (size_t)(kf + 1), slab * 8, cudaMemcpyHostToDevice, c->stream));
+    fortran_to_native<<<c->nsm * 4, 256, 0, c->stream>>>(c->dStage, c->dU, nbmax, ns, c->neq, kf);
+    WX_LAUNCHED();
+  }
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  c->dt_valid = false;
+  c->prestep = false;
+  return WX_OK;
+}
+
+int wx3d_download_U_fortran(wx_ctx* c, int32_t nbmax, double* U) {
+  if (!c || !U || nbmax <= 0) return WX_ERR_INVALID_ARG;
+  const int ns = std::min(nbmax, c->max_blocks);
+  const size_t slab = (size_t)nbmax * c->neq * 400;
+  int rc;
+  if ((rc = ensure_stage(c, slab * 8))) return rc;
+  for (int kf = 1; kf <= NC; ++kf) {
+    // keep the ghost and unused entries of the caller's slab
+    WX_CUDA(cudaMemcpyAsync(c->dStage, U + slab * (size_t)(kf + 1), slab * 8, cudaMemcpyHostToDevice, c->stream));
+    native_to_fortran<<<c->nsm * 4, 256, 0, c->stream>>>(c->dU, c->dStage, nbmax, ns, c->neq, kf);
+    WX_LAUNCHED();
+    WX_CUDA(cudaMemcpyAsync(U + slab * (size_t)(kf + 1), c->dStage, slab * 8, cudaMemcpyDeviceToHost, c->stream));
+  }
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  return WX_OK;
+}
+
+int wx3d_update_prims(wx_ctx* c) {
+  if (!ready(c)) return fail(c, WX_ERR_MESH, "no mesh");
+  if (!c->dPrim) WX_CUDA(cudaMalloc(&c->dPrim, (size_t)c->max_blocks * c->neq * BCELLS * 8));
+  c->k.prims<<<grid_for(c, (const void*)c->k.prims, 256, 0, c->nwork), 256, 0, c->stream>>>(c->dU, c->dPrim, c->dWork,
+                                                                                              c->nwork, c->dCtl, c->ph.cv);
+  WX_LAUNCHED();
+  return sync_check(c);
+}
+
+int wx3d_download_prims(wx_ctx* c, int32_t nslots, double* prim) {
+  if (!c || !prim || nslots < 0 || nslots > c->max_blocks || !c->dPrim) return WX_ERR_INVALID_ARG;
+  WX_CUDA(cudaMemcpyAsync(prim, c->dPrim, (size_t)nslots * c->neq * BCELLS * 8, cudaMemcpyDeviceToHost, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  return WX_OK;
+}
+
+int wx3d_set_state(wx_ctx* c, const wx_state* s) {
+  if (!c || !s) return WX_ERR_INVALID_ARG;
+  WX_CUDA(cudaMemcpyAsync(c->hCtl, c->dCtl, sizeof(DevCtl), cudaMemcpyDeviceToHost, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  c->hCtl->time = s->time;
+  c->hCtl->dt = s->dt;
+  c->hCtl->it = s->it;
+  c->hCtl->nextout = s->nextout;
+  c->hCtl->dumpout = s->dumpout;
+  WX_CUDA(cudaMemcpyAsync(c->dCtl, c->hCtl, sizeof(DevCtl), cudaMemcpyHostToDevice, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  return WX_OK;
+}
+
+int wx3d_get_state(wx_ctx* c, wx_state* s) {
+  if (!c || !s) return WX_ERR_INVALID_ARG;
+  WX_CUDA(cudaMemcpyAsync(c->hCtl, c->dCtl, sizeof(DevCtl), cudaMemcpyDeviceToHost, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  s->time = c->hCtl->time;
+  s->dt = c->hCtl->dt;
+  s->it = c->hCtl->it;
+  s->nextout = c->hCtl->nextout;
+  s->dumpout = c->hCtl->dumpout;
+  s->pad = c->hCtl->dumps;
+  return WX_OK;
+}
+
+int wx3d_get_timestep(wx_ctx* c, double* dt_glob) {
+  if (!ready(c) || !dt_glob) return WX_ERR_INVALID_ARG;
+  int rc;
+  if (!c->dt_valid) {
+    if ((rc = launch_dt(c, c->dU))) return rc;
+    c->dt_valid = true;
+  }
+  WX_CUDA(cudaMemcpyAsync(c->hCtl, c->dCtl, sizeof(DevCtl), cudaMemcpyDeviceToHost, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  const DevCtl& h = *c->hCtl;
+  double dt_hydro;
+  std::memcpy(&dt_hydro, &h.dtmin_bits, 8);
+  double dt_loc = c->cfg.cooling_type == WX_COOL_NONE ? dt_hydro * c->cfg.cfl : std::min(dt_hydro, 1.0e30) * c->cfg.cfl;
+  if (h.it <= 10) dt_loc = std::ldexp(1.0, -(11 - h.it)) * dt_loc;
+  const double tnext = (double)h.nextout * c->cfg.dtout / c->ph.t_sc;
+  if (h.time + dt_loc >= tnext) dt_loc = tnext - h.time;
+  *dt_glob = dt_loc;
+  return WX_OK;
+}
+
+int wx3d_hydro_solver(wx_ctx* c) {
+  if (!ready(c)) return fail(c, WX_ERR_MESH, "no mesh");
+  int rc;
+  if (!c->dt_valid) {
+    if ((rc = launch_dt(c, c->dU))) return rc;
+    c->dt_valid = true;
+  }
+  if ((rc = enqueue_solver(c, false, false))) return rc;
+  return sync_check(c);
+}
+
+int wx3d_update_neutral_fraction(wx_ctx* c) {
+  if (!ready(c)) return fail(c, WX_ERR_MESH, "no mesh");
+  if (c->cfg.eos_type != WX_EOS_H_RATE) return WX_OK;
+  int rc;
+  if (!c->dPrim && (rc = wx3d_update_prims(c))) return rc;
+  if ((rc = enqueue_sources(c, 1 | 4 | (c->cfg.cooling_type == WX_COOL_NONE ? 8 : 0)))) return rc;
+  return sync_check(c);
+}
+
+int wx3d_cooling(wx_ctx* c, double* maxloss) {
+  if (!ready(c)) return fail(c, WX_ERR_MESH, "no mesh");
+  int rc;
+  if (c->cfg.cooling_type != WX_COOL_NONE) {
+    if (!c->dPrim && (rc = wx3d_update_prims(c))) return rc;
+    WX_CUDA(cudaMemsetAsync(&c->dCtl->maxloss_bits, 0, 8, c->stream));
+    if ((rc = enqueue_sources(c, 2 | 4 | 8))) return rc;
+  }
+  if ((rc = sync_check(c))) return rc;
+  if (maxloss) std::memcpy(maxloss, &c->hCtl->maxloss_bits, 8);
+  return WX_OK;
+}
+
+int wx3d_step(wx_ctx* c, wx_state* out) {
+  if (!ready(c)) return fail(c, WX_ERR_MESH, "no mesh");
+  const int dumps0 = c->hCtl->dumps;
+  int rc;
+  c->nev = 0;
+  if ((rc = enqueue_step(c))) return rc;
+  if ((rc = sync_check(c))) return rc;
+  if (out) {
+    const DevCtl& h = *c->hCtl;
+    out->time = h.time; out->dt = h.dt; out->it = h.it; out->nextout = h.nextout;
+    out->dumpout = h.dumps != dumps0; out->pad = h.dumps;
+  }
+  return WX_OK;
+}
+
+int wx3d_run_async(wx_ctx* c, int32_t nsteps) {
+  if (!ready(c) || nsteps < 0) return WX_ERR_INVALID_ARG;
+  int rc;
+  if (!c->dt_valid) {
+    if ((rc = launch_dt(c, c->dU))) return rc;
+    c->dt_valid = true;
+  }
+  int done = 0;
+  if (nsteps >= 2) {
+    if (!c->graph_valid) {
+      // two steps bring U back to the same buffer, so one graph serves every replay
+      double* u0 = c->dU;
+      cudaGraph_t g;
+      const long long l0 = c->launches;
+      c->nev = 0;
+      WX_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      int r1 = enqueue_step(c);
+      int r2 = r1 ? r1 : enqueue_step(c);
+      cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+      c->launches = l0;
+      if (r2) return r2;
+      if (ce != cudaSuccess) return fail(c, WX_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+      if (c->dU != u0) return fail(c, WX_ERR_GENERIC, "graph capture did not return U to its buffer");
+      ce = cudaGraphInstantiate(&c->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess) return fail(c, WX_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+      c->graph_valid = true;
+    }
+    // kernels per step: step_begin, stage(s), viscous, step_end, [dt reset, sources]
+    const long long per2 = 2 * (3 + (c->cfg.solver_type == WX_SOLVER_LAX || c->cfg.solver_type == WX_SOLVER_HLL1 ? 1 : 2) +
+                                (sources_on(c) ? 2 : 0));
+    for (; done + 2 <= nsteps; done += 2) {
+      WX_CUDA(cudaGraphLaunch(c->graph, c->stream));
+      c->launches += per2;
+    }
+    c->prestep = true;
+    c->dt_valid = true;
+  }
+  // an odd remainder runs eagerly; its kernels are not timed so the event
+  // pairs keep describing the last graph replay
+  c->timing_mute = done > 0;
+  if (done == 0) c->nev = 0;
+  for (; done < nsteps; ++done)
+    if ((rc = enqueue_step(c))) { c->timing_mute = false; return rc; }
+  c->timing_mute = false;
+  return WX_OK;
+}
+
+int wx3d_run(wx_ctx* c, int32_t nsteps, wx_state* out) {
+  int rc;
+  if ((rc = wx3d_run_async(c, nsteps))) return rc;
+  if ((rc = sync_check(c))) return rc;
+  if (out) {
+    const DevCtl& h = *c->hCtl;
+    out->time = h.time; out->dt = h.dt; out->it = h.it; out->nextout = h.nextout;
+    out->dumpout = 0; out->pad = h.dumps;
+  }
+  return WX_OK;
+}
+
+int wx3d_set_cooltable(wx_ctx* c, int32_t npts, const double* logT, const double* b) {
+  if (!c || !logT || !b) return WX_ERR_INVALID_ARG;
+  if (npts < 2) return fail(c, WX_ERR_COOLING_LOAD_COEFS, "cooling table needs at least two rows");
+  std::vector<double> h(2 * (size_t)npts);
+  for (int i = 0; i < npts; ++i) {
+    if (i && !(logT[i] > logT[i - 1])) return fail(c, WX_ERR_COOLING_LOAD_COEFS, "cooling table temperatures must increase");
+    h[i] = logT[i];
+    h[npts + i] = -b[i];  // cooltable(2,i) = -b (cooling.f90:163)
+  }
+  cudaFree(c->dCool);
+  c->dCool = nullptr;
+  WX_CUDA(cudaMalloc(&c->dCool, h.size() * 8));
+  WX_CUDA(cudaMemcpy(c->dCool, h.data(), h.size() * 8, cudaMemcpyHostToDevice));
+  c->ncool = npts;
+  invalidate_graph(c);
+  return WX_OK;
+}
+
+int wx3d_mark(wx_ctx* c, int32_t nslots, int32_t* flags) {
+  if (!ready(c) || !flags || nslots > c->max_blocks) return WX_ERR_INVALID_ARG;
+  WX_CUDA(cudaMemsetAsync(c->dFlags, 0xff, 4 * (size_t)c->max_blocks, c->stream));
+  MarkParams P{c->dU, c->prestep ? c->dW : c->dU, c->dBlocks, c->dWork, c->nwork, c->dFlags, c->cfg.maxlev,
+               c->cfg.refine_thres, c->cfg.coarse_thres, c->ph};
+  c->k.mark<<<grid_for(c, (const void*)c->k.mark, 256, 0, c->nwork), 256, 0, c->stream>>>(P);
+  WX_LAUNCHED();
+  WX_CUDA(cudaMemcpyAsync(flags, c->dFlags, 4 * (size_t)nslots, cudaMemcpyDeviceToHost, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  return WX_OK;
+}
+
+int wx3d_refine(wx_ctx* c, int32_t father, const int32_t* ch) {
+  if (!c || !ch || father < 0 || father >= c->max_blocks) return WX_ERR_INVALID_ARG;
+  Slots8 s;
+  for (int i = 0; i < 8; ++i) {
+    if (ch[i] < 0 || ch[i] >= c->max_blocks || ch[i] == father) return WX_ERR_INVALID_ARG;
+    s.s[i] = ch[i];
+  }
+  refine_kernel<<<dim3(16, 8), 256, 0, c->stream>>>(c->dU, c->neq, father, s);
+  WX_LAUNCHED();
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  c->dt_valid = false;
+  c->prestep = false;
+  invalidate_graph(c);
+  return WX_OK;
+}
+
+int wx3d_coarsen(wx_ctx* c, const int32_t* ch, int32_t father) {
+  if (!c || !ch || father < 0 || father >= c->max_blocks) return WX_ERR_INVALID_ARG;
+  Slots8 s;
+  for (int i = 0; i < 8; ++i) {
+    if (ch[i] < 0 || ch[i] >= c->max_blocks || ch[i] == father) return WX_ERR_INVALID_ARG;
+    s.s[i] = ch[i];
+  }
+  coarsen_kernel<<<dim3(4, 8), 256, 0, c->stream>>>(c->dU, c->neq, father, s);
+  WX_LAUNCHED();
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  c->dt_valid = false;
+  c->prestep = false;
+  invalidate_graph(c);
+  return WX_OK;
+}
+
+int wx3d_set_timing(wx_ctx* c, int32_t on) {
+  if (!c) return WX_ERR_INVALID_ARG;
+  if (on && !c->ev[0])
+    for (int i = 0; i < 64; ++i) WX_CUDA(cudaEventCreate(&c->ev[i]));
+  c->timing = on != 0;
+  c->nev = 0;
+  invalidate_graph(c);
+  return WX_OK;
+}
+
+int wx3d_kernel_times(wx_ctx* c, double* ms4, int32_t* count4) {
+  if (!c || !ms4) return WX_ERR_INVALID_ARG;
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < 4; ++k) { ms4[k] = 0.0; if (count4) count4[k] = 0; }
+  for (int p = 0; p + 1 < c->nev; p += 2) {
+    float ms = 0.f;
+    WX_CUDA(cudaEventElapsedTime(&ms, c->ev[p], c->ev[p + 1]));
+    const int k = c->ev_kind[p / 2];
+    ms4[k] += ms;
+    if (count4) ++count4[k];
+  }
+  return WX_OK;
+}
+
+int wx3d_get_status(wx_ctx* c, wx_status* st) {
+  if (!c || !st) return WX_ERR_INVALID_ARG;
+  WX_CUDA(cudaMemcpyAsync(c->hCtl, c->dCtl, sizeof(DevCtl), cudaMemcpyDeviceToHost, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  st->pressure_floor = (int64_t)c->hCtl->cnt[0];
+  st->density_floor = (int64_t)c->hCtl->cnt[1];
+  st->zero_density = (int64_t)c->hCtl->cnt[2];
+  st->nan_cells = (int64_t)c->hCtl->cnt[3];
+  std::memcpy(&st->max_cool_loss, &c->hCtl->maxloss_bits, 8);
+  st->kernels_launched = c->launches;
+  return WX_OK;
+}
+
+int wx3d_reset_status(wx_ctx* c) {
+  if (!c) return WX_ERR_INVALID_ARG;
+  WX_CUDA(cudaMemsetAsync(&c->dCtl->cnt[0], 0, sizeof(c->hCtl->cnt) + 8, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  return WX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,440 @@
+// wx3d_kernels.cuh -- sm_100a kernels of the per-block Godunov update.
+//
+// Stage kernel: one CTA per (block, z-slab).  288 threads (9 warps) march
+// through the slab's k-planes; a 4-plane shared-memory ring holds the
+// primitives of each plane together with its two-deep x/y ghost frame, so
+// every x-, y- and z-interface flux is computed exactly once and the
+// conservative update (godunov.f90:259-271) reads the two fluxes of each
+// face from shared memory (x, y) or from the thread's registers (z).
+#pragma once
+
+#include "wx3d_device.cuh"
+
+namespace wx {
+
+constexpr int STAGE_THREADS = 288;  // 17*16 x- and y-interfaces per plane
+constexpr int RING = 4;             // planes p-1..p+2 of the second-order stencil
+
+struct StageParams {
+  const double* __restrict__ src;   // array whose primitives feed the fluxes
+  const double* __restrict__ base;  // array the update starts from (U)
+  double* __restrict__ out;         // result (UP for stage 1, W for stage 2)
+  const DevBlock* __restrict__ blocks;
+  const int32_t* __restrict__ work; // occupied slots
+  int32_t nwork;                    // number of (block, slab) items
+  int32_t zsplit;                   // slabs per block (1, 2, 4 or 8)
+  DevCtl* ctl;
+  double dt_factor;                 // 0.5 for the predictor, 1 otherwise
+  PhysParams ph;
+};
+
+template <int NEQ>
+constexpr size_t stage_smem_bytes() {
+  return sizeof(double) * ((size_t)RING * NEQ * HPLANE + 2 * (size_t)NEQ * 17 * NC) + sizeof(DevBlock);
+}
+
+__device__ __forceinline__ int hidx(int i, int j) { return (i + 1) + HW * (j + 1); }
+__device__ __forceinline__ int ring_slot(int kk) { return (kk + 64) & (RING - 1); }
+
+// Block-wide sum of four status counters into ctl->cnt.
+__device__ __forceinline__ void flush_counts(DevCtl* ctl, unsigned pf, unsigned df, unsigned zd) {
+  unsigned m = __activemask();
+  pf = __reduce_add_sync(m, pf);
+  df = __reduce_add_sync(m, df);
+  zd = __reduce_add_sync(m, zd);
+  if ((threadIdx.x & 31) == 0) {
+    if (pf) atomicAdd(&ctl->cnt[0], (unsigned long long)pf);
+    if (df) atomicAdd(&ctl->cnt[1], (unsigned long long)df);
+    if (zd) atomicAdd(&ctl->cnt[2], (unsigned long long)zd);
+  }
+}
+
+// One interface flux in direction DIR from ring cells c0..c3 (pointers to
+// equation 0 of cells l-1, l, r, r+1; stride HPLANE between equations).
+template <int NEQ, bool MHD, int SOLVER, int ORDER, int DIR>
+__device__ __forceinline__ void iface_flux(const double* c0, const double* c1, const double* c2, const double* c3,
+                                           const PhysParams& ph, double* f) {
+  double pl[NEQ], pr[NEQ], fx[NEQ];
+#pragma unroll
+  for (int e = 0; e < NEQ; ++e) {
+    const int q = perm<DIR, MHD>(e);
+    pl[e] = c1[q * HPLANE];
+    pr[e] = c2[q * HPLANE];
+  }
+  if (ORDER == 2) {  // limiter (hydro_core.f90:613-636) on permuted primitives
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) {
+      const int q = perm<DIR, MHD>(e);
+      const double pll = c0[q * HPLANE], prr = c3[q * HPLANE];
+      const double dl = pl[e] - pll, dm = pr[e] - pl[e], dr = prr - pr[e];
+      const double al = average(dl, dm, ph.limiter);
+      const double ar = average(dm, dr, ph.limiter);
+      pl[e] = pl[e] + 0.5 * al;
+      pr[e] = pr[e] - 0.5 * ar;
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < NEQ; ++e) fx[e] = 0.0;
+  riemann<NEQ, MHD, SOLVER>(pl, pr, fx, ph.gamma, ph.cv);
+#pragma unroll
+  for (int e = 0; e < NEQ; ++e) f[perm<DIR, MHD>(e)] = fx[e];
+}
+
+template <int NEQ, bool MHD, int SOLVER, int ORDER>
+__global__ void __launch_bounds__(STAGE_THREADS) stage_kernel(StageParams P) {
+  extern __shared__ __align__(16) double smem[];
+  double* ring = smem;                                   // [RING][NEQ][HPLANE]
+  double* fxs = ring + RING * NEQ * HPLANE;              // [NEQ][16 rows][17]
+  double* fys = fxs + NEQ * 17 * NC;                     // [NEQ][17][16 cols]
+  DevBlock& B = *reinterpret_cast<DevBlock*>(fys + NEQ * 17 * NC);
+  const int t = threadIdx.x;
+  const int planes = NC / P.zsplit;
+  const PhysParams& ph = P.ph;
+  const double dtp = P.ctl->dt * P.dt_factor;
+  unsigned pf = 0, df = 0, zd = 0;
+
+  for (int w = blockIdx.x; w < P.nwork; w += gridDim.x) {
+    const int slot = P.work[w / P.zsplit];
+    const int z0 = 1 + (w % P.zsplit) * planes, z1 = z0 + planes - 1;
+    __syncthreads();
+    if (t < (int)(sizeof(DevBlock) / 4)) reinterpret_cast<int*>(&B)[t] = reinterpret_cast<const int*>(P.blocks + slot)[t];
+    __syncthreads();
+    const double dtdx = dtp / B.dx, dtdy = dtp / B.dy, dtdz = dtp / B.dz;
+    const int ci = (t & (NC - 1)) + 1, cj = (t >> 4) + 1;   // column of threads t < 256
+    double zprev[NEQ], znew[NEQ];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) { zprev[e] = 0.0; znew[e] = 0.0; }
+
+    for (int kk = z0 - ORDER; kk <= z1 + ORDER; ++kk) {
+      // ---- load plane kk into the ring (conserved -> primitive) ----------
+      __syncthreads();
+      {
+        double* pl = ring + ring_slot(kk) * NEQ * HPLANE;
+        const bool inner = (kk >= 1 && kk <= NC);
+        const bool frame = (kk >= z0 && kk <= z1);  // plane gets x/y fluxes
+        const int nframe = frame ? (ORDER == 2 ? 128 : 64) : 0;
+        for (int c = t; c < PLANE + nframe; c += STAGE_THREADS) {
+          int i, j;
+          if (c < PLANE) { i = (c & 15) + 1; j = (c >> 4) + 1; }
+          else {
+            const int h = c - PLANE;
+            const int per = ORDER == 2 ? 32 : 16;         // cells per side
+            const int side = h / per, r = (h % 16) + 1;
+            const int d = (ORDER == 2) ? ((h % 32) >> 4) : 1;   // 0: outer, 1: inner ghost layer
+            if (side == 0) { i = d - 1; j = r; }
+            else if (side == 1) { i = NC + 2 - d; j = r; }
+            else if (side == 2) { i = r; j = d - 1; }
+            else { i = r; j = NC + 2 - d; }
+          }
+          double u[NEQ], p[NEQ];
+          if (inner) get_cell<NEQ>(P.src, B, slot, ph.bc, i, j, kk, u);
+          else gather_ghost<NEQ>(P.src, B, slot, ph.bc, i, j, kk, u);
+          const int st = flow2prim<NEQ, MHD>(u, p, ph.cv);
+          if (c < PLANE && inner && frame) {
+            pf += (st == 1);
+            df += (st == 2);
+            zd += (st < 0);
+          }
+#pragma unroll
+          for (int e = 0; e < NEQ; ++e) pl[e * HPLANE + hidx(i, j)] = p[e];
+        }
+      }
+      __syncthreads();
+      const int m = kk - ORDER;  // z-interface m+1/2 and update plane p = m
+      // ---- z-interface m+1/2 of column t ---------------------------------
+      if (m >= z0 - 1 && t < PLANE) {
+        const int h = hidx(ci, cj);
+        const double* c0 = ring + ring_slot(m - 1) * NEQ * HPLANE + h;
+        const double* c1 = ring + ring_slot(m) * NEQ * HPLANE + h;
+        const double* c2 = ring + ring_slot(m + 1) * NEQ * HPLANE + h;
+        const double* c3 = ring + ring_slot(m + 2) * NEQ * HPLANE + h;
+        iface_flux<NEQ, MHD, SOLVER, ORDER, 2>(c0, c1, c2, c3, ph, znew);
+      }
+      const bool upd = (m >= z0 && m <= z1);
+      if (upd && t < 17 * NC) {
+        const double* pp = ring + ring_slot(m) * NEQ * HPLANE;
+        {  // x-interface between ii and ii+1 in row jx
+          const int ii = t % 17, jx = t / 17 + 1;
+          double f[NEQ];
+          iface_flux<NEQ, MHD, SOLVER, ORDER, 0>(pp + hidx(ii - 1, jx), pp + hidx(ii, jx), pp + hidx(ii + 1, jx),
+                                                 pp + hidx(ii + 2, jx), ph, f);
+#pragma unroll
+          for (int e = 0; e < NEQ; ++e) fxs[(e * NC + (jx - 1)) * 17 + ii] = f[e];
+        }
+        {  // y-interface between jj and jj+1 in column iy
+          const int iy = (t & 15) + 1, jj = t >> 4;
+          double f[NEQ];
+          iface_flux<NEQ, MHD, SOLVER, ORDER, 1>(pp + hidx(iy, jj - 1), pp + hidx(iy, jj), pp + hidx(iy, jj + 1),
+                                                 pp + hidx(iy, jj + 2), ph, f);
+#pragma unroll
+          for (int e = 0; e < NEQ; ++e) fys[(e * 17 + jj) * NC + (iy - 1)] = f[e];
+        }
+      }
+      __syncthreads();
+      // ---- conservative update of plane m (godunov.f90:259-271) ----------
+      if (upd && t < PLANE) {
+        double s[NEQ];
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) s[e] = 0.0;
+        if (MHD && ph.eight_wave) {  // Powell source (sources.f90:38-95) on the stage primitives
+          const double* pm = ring + ring_slot(m) * NEQ * HPLANE;
+          const double* pd = ring + ring_slot(m - 1) * NEQ * HPLANE;
+          const double* pu = ring + ring_slot(m + 1) * NEQ * HPLANE;
+          const int h = hidx(ci, cj);
+          const double divB = (pm[5 * HPLANE + h + 1] - pm[5 * HPLANE + h - 1]) / (2. * B.dx) +
+                              (pm[6 * HPLANE + h + HW] - pm[6 * HPLANE + h - HW]) / (2. * B.dy) +
+                              (pu[7 * HPLANE + h] - pd[7 * HPLANE + h]) / (2. * B.dz);
+          const double v1 = pm[1 * HPLANE + h], v2 = pm[2 * HPLANE + h], v3 = pm[3 * HPLANE + h];
+          const double b1 = pm[5 * HPLANE + h], b2 = pm[6 * HPLANE + h], b3 = pm[7 * HPLANE + h];
+          s[1] = -divB * b1;
+          s[2] = -divB * b2;
+          s[3] = -divB * b3;
+          s[4] = -divB * (v1 * b1 + v2 * b2 + v3 * b3);
+          s[5] = -divB * v1;
+          s[6] = -divB * v2;
+          s[7] = -divB * v3;
+        }
+        const size_t o = cell_off(slot, NEQ, 0, ci, cj, m);
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) {
+          const double fxl = fxs[(e * NC + (cj - 1)) * 17 + ci - 1], fxr = fxs[(e * NC + (cj - 1)) * 17 + ci];
+          const double fyl = fys[(e * 17 + cj - 1) * NC + ci - 1], fyr = fys[(e * 17 + cj) * NC + ci - 1];
+          double v = __ldg(P.base + o + (size_t)e * BCELLS) + dtdx * (fxl - fxr) + dtdy * (fyl - fyr) +
+                     dtdz * (zprev[e] - znew[e]);
+          if (MHD && ph.eight_wave) v = v + dtp * s[e];
+          P.out[o + (size_t)e * BCELLS] = v;
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e) zprev[e] = znew[e];
+    }
+  }
+  flush_counts(P.ctl, pf, df, zd);
+}
+
+// ---------------------------------------------------------------------------
+// Lax-Friedrichs (lax.f90:39-99): first order, from U with one-deep ghosts.
+struct LaxParams {
+  const double* __restrict__ u;
+  double* __restrict__ out;
+  const DevBlock* __restrict__ blocks;
+  const int32_t* __restrict__ work;
+  int32_t nwork;
+  DevCtl* ctl;
+  PhysParams ph;
+};
+
+template <int NEQ, bool MHD>
+__global__ void __launch_bounds__(256) lax_kernel(LaxParams P) {
+  __shared__ DevBlock B;
+  const int t = threadIdx.x;
+  const int i = (t & 15) + 1, j = (t >> 4) + 1;
+  for (int w = blockIdx.x; w < P.nwork; w += gridDim.x) {
+    const int slot = P.work[w];
+    __syncthreads();
+    if (t < (int)(sizeof(DevBlock) / 4)) reinterpret_cast<int*>(&B)[t] = reinterpret_cast<const int*>(P.blocks + slot)[t];
+    __syncthreads();
+    const double dt = P.ctl->dt;
+    const double cx = 0.5 * dt / B.dx, cy = 0.5 * dt / B.dy, cz = 0.5 * dt / B.dz;
+    for (int k = 1; k <= NC; ++k) {
+      double un[6][NEQ], fl[NEQ], fr[NEQ], pv[NEQ], tmp[NEQ];
+      const int di[6] = {1, -1, 0, 0, 0, 0}, dj[6] = {0, 0, 1, -1, 0, 0}, dk[6] = {0, 0, 0, 0, 1, -1};
+#pragma unroll
+      for (int q = 0; q < 6; ++q) get_cell<NEQ>(P.u, B, slot, P.ph.bc, i + di[q], j + dj[q], k + dk[q], un[q]);
+      double res[NEQ];
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e)
+        res[e] = (un[0][e] + un[1][e] + un[2][e] + un[3][e] + un[4][e] + un[5][e]) / 6.0;
+      // physical fluxes of the neighbour primitives, direction by direction
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double cc = d == 0 ? cx : (d == 1 ? cy : cz);
+        flow2prim<NEQ, MHD>(un[2 * d], pv, P.ph.cv);
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) tmp[e] = pv[d == 0 ? e : (d == 1 ? perm<1, MHD>(e) : perm<2, MHD>(e))];
+        xflux<NEQ, MHD>(tmp, fr, P.ph.cv);
+        flow2prim<NEQ, MHD>(un[2 * d + 1], pv, P.ph.cv);
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) tmp[e] = pv[d == 0 ? e : (d == 1 ? perm<1, MHD>(e) : perm<2, MHD>(e))];
+        xflux<NEQ, MHD>(tmp, fl, P.ph.cv);
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) {
+          const int q = d == 0 ? e : (d == 1 ? perm<1, MHD>(e) : perm<2, MHD>(e));
+          res[q] = res[q] - cc * (fr[e] - fl[e]);
+        }
+      }
+      const size_t o = cell_off(slot, NEQ, 0, i, j, k);
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e) P.out[o + (size_t)e * BCELLS] = res[e];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// doViscousStep (hydro_solver.f90:217-250) with the next step's CFL minimum
+// (hydro_solver.f90:150-182) of the new state fused into the epilogue.
+struct ViscParams {
+  double* __restrict__ w;              // stage result, overwritten in place by U^{n+1}
+  const double* __restrict__ up;       // predictor state: source of the face ghosts
+  const DevBlock* __restrict__ blocks;
+  const int32_t* __restrict__ work;
+  int32_t nwork;
+  int32_t zero_ghost;                  // single-stage solvers: UP ghosts are never filled (0)
+  int32_t do_dt;                       // fold the CFL minimum of the new state
+  DevCtl* ctl;
+  PhysParams ph;
+};
+
+__device__ __forceinline__ void block_min_dt(double v, DevCtl* ctl) {
+  v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 16));
+  v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 8));
+  v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 4));
+  v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 2));
+  v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 1));
+  if ((threadIdx.x & 31) == 0) atomic_min_pos(&ctl->dtmin_bits, v);
+}
+
+template <int NEQ, bool MHD>
+__global__ void __launch_bounds__(256) viscous_kernel(ViscParams P) {
+  __shared__ DevBlock B;
+  __shared__ double pl[NEQ][18 * 18];   // plane k of W with the one-deep ghost frame from UP
+  const int t = threadIdx.x;
+  const int i = (t & 15) + 1, j = (t >> 4) + 1;
+  const double eta = P.ph.eta;
+  double dtl = 1.0e300;
+  unsigned nonfinite = 0;
+  auto q = [](int ii, int jj) { return ii + 18 * jj; };
+  for (int w = blockIdx.x; w < P.nwork; w += gridDim.x) {
+    const int slot = P.work[w];
+    __syncthreads();
+    if (t < (int)(sizeof(DevBlock) / 4)) reinterpret_cast<int*>(&B)[t] = reinterpret_cast<const int*>(P.blocks + slot)[t];
+    __syncthreads();
+    double wm[NEQ], wc[NEQ], wp[NEQ];
+    // W(k-1) for k=1 is the bottom ghost of UP
+    if (P.zero_ghost) {
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e) wm[e] = 0.0;
+    } else {
+      gather_ghost<NEQ>(P.up, B, slot, P.ph.bc, i, j, 0, wm);
+    }
+    load_cell_rw<NEQ>(P.w, slot, i, j, 1, wc);
+    for (int k = 1; k <= NC; ++k) {
+      if (k < NC) load_cell_rw<NEQ>(P.w, slot, i, j, k + 1, wp);
+      else if (P.zero_ghost) {
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) wp[e] = 0.0;
+      } else {
+        gather_ghost<NEQ>(P.up, B, slot, P.ph.bc, i, j, NC + 1, wp);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e) pl[e][q(i, j)] = wc[e];
+      if (t < 64) {  // one-deep x/y ghost frame of plane k from UP
+        const int side = t >> 4, r = (t & 15) + 1;
+        int gi, gj;
+        if (side == 0) { gi = 0; gj = r; }
+        else if (side == 1) { gi = NC + 1; gj = r; }
+        else if (side == 2) { gi = r; gj = 0; }
+        else { gi = r; gj = NC + 1; }
+        double g[NEQ];
+        if (P.zero_ghost) {
+#pragma unroll
+          for (int e = 0; e < NEQ; ++e) g[e] = 0.0;
+        } else {
+          gather_ghost<NEQ>(P.up, B, slot, P.ph.bc, gi, gj, k, g);
+        }
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) pl[e][q(gi, gj)] = g[e];
+      }
+      __syncthreads();
+      double un[NEQ];
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e) {
+        const double c = wc[e];
+        un[e] = c + eta * (+pl[e][q(i + 1, j)] + pl[e][q(i - 1, j)] + pl[e][q(i, j + 1)] + pl[e][q(i, j - 1)] + wp[e] +
+                           wm[e] - 6.0 * c);
+      }
+      const size_t o = cell_off(slot, NEQ, 0, i, j, k);
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e) {
+        P.w[o + (size_t)e * BCELLS] = un[e];
+        nonfinite += !isfinite(un[e]);
+      }
+      if (P.do_dt) {
+        double p[NEQ];
+        flow2prim<NEQ, MHD>(un, p, P.ph.cv);
+        dtl = dmin(dtl, cell_dt<NEQ, MHD>(p, B, P.ph.gamma));
+      }
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e) { wm[e] = wc[e]; wc[e] = wp[e]; }
+    }
+  }
+  if (P.do_dt) block_min_dt(dtl, P.ctl);
+  nonfinite = __reduce_add_sync(0xffffffffu, nonfinite);
+  if ((t & 31) == 0 && nonfinite) atomicAdd(&P.ctl->cnt[3], (unsigned long long)nonfinite);
+}
+
+// CFL minimum of an arbitrary state (getTimestep's loop, hydro_solver.f90:150-182).
+struct DtParams {
+  const double* __restrict__ u;
+  const DevBlock* __restrict__ blocks;
+  const int32_t* __restrict__ work;
+  int32_t nwork;
+  DevCtl* ctl;
+  PhysParams ph;
+};
+
+template <int NEQ, bool MHD>
+__global__ void __launch_bounds__(256) dt_kernel(DtParams P) {
+  const int t = threadIdx.x;
+  double dtl = 1.0e300;
+  for (int w = blockIdx.x; w < P.nwork; w += gridDim.x) {
+    const int slot = P.work[w];
+    const DevBlock& B = P.blocks[slot];
+    for (int k = 1; k <= NC; ++k) {
+      double u[NEQ], p[NEQ];
+      load_cell<NEQ>(P.u, slot, (t & 15) + 1, (t >> 4) + 1, k, u);
+      flow2prim<NEQ, MHD>(u, p, P.ph.cv);
+      dtl = dmin(dtl, cell_dt<NEQ, MHD>(p, B, P.ph.gamma));
+    }
+  }
+  block_min_dt(dtl, P.ctl);
+}
+
+__global__ void ctl_reset_dtmin_kernel(DevCtl* ctl) {
+  if (threadIdx.x == 0) ctl->dtmin_bits = (unsigned long long)__double_as_longlong(1.0e30);
+}
+
+// getTimestep's scalar tail (hydro_solver.f90:185-207) and the iteration
+// counter of main.f90:81.  Single thread.
+__global__ void step_begin_kernel(DevCtl* ctl, double cfl, int cooling_on, double dtout, double t_sc, int bump_it) {
+  if (threadIdx.x != 0) return;
+  if (bump_it) ctl->it = ctl->it + 1;
+  const double dt_hydro = __longlong_as_double((long long)ctl->dtmin_bits);
+  const double dt_cool = 1.0e30;
+  double dt_loc = cooling_on ? dmin(dt_hydro, dt_cool) * cfl : dt_hydro * cfl;
+  if (ctl->it <= 10) dt_loc = exp2(-(double)(11 - ctl->it)) * dt_loc;
+  double dt_glob = dt_loc;
+  const double tnext = (double)ctl->nextout * dtout / t_sc;
+  if (ctl->time + dt_glob >= tnext) {
+    dt_glob = tnext - ctl->time;
+    ctl->dumpout = 1;
+  }
+  ctl->dt = dt_glob;
+  ctl->dtmin_bits = (unsigned long long)__double_as_longlong(1.0e30);
+}
+
+// time += dt (hydro_solver.f90:225) and, when the call stands for a whole
+// main-loop iteration, the output bookkeeping of main.f90:109-114 (the
+// output itself belongs to the host).
+__global__ void step_end_kernel(DevCtl* ctl, int finish_output) {
+  if (threadIdx.x != 0) return;
+  ctl->time = ctl->time + ctl->dt;
+  if (finish_output && ctl->dumpout) {
+    ctl->nextout = ctl->nextout + 1;
+    ctl->dumpout = 0;
+    ctl->dumps = ctl->dumps + 1;
+  }
+}
+
+}  // namespace wx

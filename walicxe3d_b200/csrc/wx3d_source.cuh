@@ -1,0 +1,395 @@
+// wx3d_source.cuh -- per-cell source terms (hrate.f90, cooling.f90,
+// cooling_h.f90), markByPhysical and the AMR data copies, as sm_100a kernels.
+#pragma once
+
+#include "wx3d_device.cuh"
+
+namespace wx {
+
+constexpr double AMU = 1.660538782e-24;  // source/constants.f90:37
+constexpr double KB = 1.380650400e-16;   // source/constants.f90:38
+
+// calcTemp (hydro_core.f90:231-270)
+template <int FP>
+__device__ __forceinline__ double calc_temp(const double* p, const PhysParams& ph) {
+  double temp = 0.0;
+  switch (ph.eos) {
+    case WX_EOS_ADIABATIC:
+    case WX_EOS_SINGLE_SPECIE: temp = p[4] / p[0] * (ph.mu0 * AMU * ph.p_sc / ph.d_sc / KB); break;
+    case WX_EOS_TWOTEMP:
+      temp = p[4] / p[0] * (ph.mu0 * AMU * ph.p_sc / ph.d_sc / KB);
+      if (temp > ph.ion_thres) temp = p[4] / p[0] * (ph.mui * AMU * ph.p_sc / ph.d_sc / KB);
+      break;
+    case WX_EOS_H_RATE:
+      if (ph.npassive >= 1) temp = p[4] / (2.0 * p[0] / ph.mu0 - p[FP]) * ph.p_sc / KB;
+      break;
+  }
+  return temp;
+}
+
+// solve_h_rate for one cell (hrate.f90:96-137); returns the new neutral
+// fraction y1 for the cell's temperature T and H density dh.
+__device__ __forceinline__ double h_rate_y1(double T, double dh, double y0, double dts) {
+  const double xi = 1.e-4;
+  const double col = 5.83e-11 * sqrt(T) * exp(-157828. / T);   // colf, hrate.f90:73
+  const double rec = 2.55e-13 * pow(1.e4 / T, 0.79);          // alpha, hrate.f90:58
+  const double a = rec + col;
+  const double b = -((2.0 + xi) * rec + (1.0 + xi) * col + 0.0);
+  const double c = (1.0 + xi) * rec;
+  const double d = sqrt(b * b - 4.0 * a * c);
+  const double g0 = (2.0 * a * y0 + b + d) / (2.0 * a * y0 + b - d);
+  const double e = exp(-d * dh * dts);
+  double y1 = (-b - d * (1.0 + g0 * e) / (1.0 - g0 * e)) / (2.0 * a);
+  y1 = dmin(y1, 1.0 - xi);
+  y1 = dmax(y1, 0.0);
+  return y1;
+}
+
+// betah and aloss (cooling_h.f90:42-145), Biro et al. 1999 loss rate.
+__device__ __forceinline__ double betah(double T) {
+  const double a = 157890. / T;
+  return 1.133e-24 / sqrt(a) * (-0.0713 + 0.5 * log(a) + 0.640 * pow(a, -0.33333));
+}
+
+__device__ __forceinline__ double aloss_h(double x1, double den, double dH0, double Te0) {
+  const double XION = 2.179e-11, XO = 1.e-3;
+  const double C0 = 0.5732, C1 = 1.8288e-5, C2 = -1.15822e-10, C3 = 9.4288e-16;
+  const double D0 = 0.5856, D1 = 1.55083e-5, D2 = -9.669e-12, D3 = 5.716e-19;
+  const double ENK = 118409., EN = 1.634E-11;
+  const double Te = dmax(Te0, 10.);
+  const double dHp = (1. - x1) * den;
+  const double de = dHp + 1.E-4 * den;
+  const double dOI = XO * dH0;
+  const double dOII = XO * dHp;
+  if (Te <= 1e4) return 1e-30;
+  double omega;
+  const double oL = C0 + Te * (C1 + Te * (C2 + Te * C3));
+  const double oH = D0 + Te * (D1 + Te * (D2 + Te * D3));
+  if (Te <= 55000.) omega = oL;
+  else if (Te >= 72000.) omega = oH;
+  else {
+    const double frac = (Te - 55000.) / 17000.;
+    omega = (1. - frac) * oL + frac * oH;
+  }
+  const double sTe = sqrt(Te);
+  const double qla = 8.6287E-6 / (2. * sTe) * omega * exp(-ENK / Te);
+  const double ecoll = dmax(de * dH0 * qla * EN, 0.);
+  const double cion = 5.834E-11 * sTe * exp(-1.579E5 / Te);
+  const double eion = de * dH0 * cion * XION;
+  const double erec = dmax(de * dHp * betah(Te), 0.);
+  const double Tm = 1. / Te;
+  const double Tm2 = Tm * Tm;
+  const double eOI = dmax(de * dOI * pow(10., 1381465 * Tm2 - 12328.69 * Tm - 19.82621), 0.);
+  const double eOII = dmax(de * dOII * pow(10., -2061075. * Tm2 - 14596.24 * Tm - 19.01402), 0.);
+  const double betaf = 1.3 * 1.42E-27 * pow(Te, 0.5);
+  const double HIIcool = de * dHp * betaf;
+  const double equil = (1.0455E-18 / pow(Te, 0.63)) * (1. - exp(-pow(Te * 1.E-5, 1.63))) * de * den + HIIcool;
+  double fr;
+  if (Te <= 44770.) fr = 0.;
+  else if (Te >= 54770.) fr = 1.;
+  else {
+    const double ex2 = exp(-2. * (Te - 49770.) / 500.);
+    fr = 0.5 * (1. + (1. - ex2) / (1. + ex2));
+  }
+  return ecoll + eion + (erec + 7.033 * (eOI + eOII)) * (1. - fr) + equil * fr;
+}
+
+// find_coef (cooling.f90:378-419).  The reference scans for the first row
+// whose logT exceeds the argument; on the (increasing) table this is the
+// upper bound found here by bisection.
+__device__ __forceinline__ double find_coef(const double* __restrict__ lt, const double* __restrict__ lc, int n,
+                                            double logT) {
+  if (logT < lt[0]) return 0.0;
+  if (logT >= lt[n - 1]) return pow(10., lc[n - 1] + 0.5 * (logT - lt[n - 1]));
+  int lo = 0, hi = n - 1;  // lt[lo] <= logT < lt[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (lt[mid] > logT) hi = mid; else lo = mid;
+  }
+  const double T0 = lt[hi - 1], C0 = lc[hi - 1], T1 = lt[hi], C1 = lc[hi];
+  return pow(10., (C1 - C0) / (T1 - T0) * (logT - T0) + C0);
+}
+
+// mode bits: 1 = updateNeutralFraction, 2 = cooling, 4 = primitives come
+// from and go to the PRIM buffer (separate calls, as the reference's PRIM
+// array), otherwise they are recomputed from U (fused step); 8 = fold the
+// CFL minimum of the resulting primitives.
+struct SrcParams {
+  double* __restrict__ u;
+  double* __restrict__ prim;
+  const DevBlock* __restrict__ blocks;
+  const int32_t* __restrict__ work;
+  int32_t nwork;
+  int32_t mode;
+  DevCtl* ctl;
+  const double* __restrict__ cool_lt;   // cooltable(1,:)
+  const double* __restrict__ cool_lc;   // cooltable(2,:) (= -b)
+  int32_t ncool;
+  PhysParams ph;
+};
+
+// updatePrims + updateNeutralFraction + cooling for every physical cell
+// (main.f90:94-100), followed by the CFL minimum of the resulting PRIM.
+template <int NEQ, bool MHD>
+__global__ void __launch_bounds__(256) source_kernel(SrcParams P) {
+  constexpr int FP = MHD ? 8 : 5;
+  constexpr bool HAS_PAS = NEQ > FP;
+  const PhysParams& ph = P.ph;
+  const int t = threadIdx.x;
+  const double dts = P.ctl->dt * ph.t_sc;
+  const bool do_hrate = P.mode & 1, do_cool = P.mode & 2, use_prim = P.mode & 4, do_dt = P.mode & 8;
+  double dtl = 1.0e300, mloss = 0.0;
+  for (int w = blockIdx.x; w < P.nwork; w += gridDim.x) {
+    const int slot = P.work[w];
+    const DevBlock& B = P.blocks[slot];
+    for (int c = t; c < BCELLS; c += 256) {
+      const size_t o = ((size_t)slot * NEQ) * BCELLS + c;
+      double u[NEQ], p[NEQ];
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e) u[e] = P.u[o + (size_t)e * BCELLS];
+      if (use_prim) {
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) p[e] = P.prim[o + (size_t)e * BCELLS];
+      } else {
+        flow2prim<NEQ, MHD>(u, p, ph.cv);
+      }
+      constexpr int fp = FP;
+      if (HAS_PAS && do_hrate && ph.eos == WX_EOS_H_RATE) {  // hrate.f90:101-140
+        const double T = calc_temp<FP>(p, ph);
+        const double dh = p[0] / ph.mu0;
+        const double y0 = p[fp] / dh;
+        const double y1 = h_rate_y1(T, dh, y0, dts);
+        p[fp] = p[0] * y1 / ph.mu0;
+        if (ph.cooling != WX_COOL_H) u[fp] = p[fp];
+      }
+      if (do_cool && ph.cooling == WX_COOL_TABLE && P.ncool >= 2) {  // cooling.f90:303-369
+        const double temp = calc_temp<FP>(p, ph);
+        const double logT = log10(temp);
+        if (logT >= P.cool_lt[0]) {
+          const double ETH = ph.cv * p[4];
+          const double EK = 0.5 * p[0] * (p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
+          const double al = find_coef(P.cool_lt, P.cool_lc, P.ncool, logT);
+          const double nd = p[0] * ph.d_sc / (ph.mui * AMU);
+          const double ce = al * (nd * nd) / (ETH * ph.e_sc);
+          double cf = exp(-ce * dts);
+          mloss = dmax(mloss, 1.0 - cf);
+          if (cf < 1.0 - ph.cooling_limit) cf = 1.0 - ph.cooling_limit;
+          if (temp * cf < 10.0) cf = 10.0 / temp;
+          p[4] = p[4] * cf;
+          u[4] = EK + ph.cv * p[4];
+        }
+      } else if (HAS_PAS && do_cool && ph.cooling == WX_COOL_H) {  // cooling_h.f90:175-246
+        const double dh = p[0] / ph.mu0;
+        const double dh0 = p[fp];
+        const double y0 = ph.mu0 * u[fp] / u[0];
+        u[fp] = p[fp];
+        const double Temp = calc_temp<FP>(p, ph);
+        if (Temp > 1.e4) {
+          const double L0 = aloss_h(y0, dh, dh0, Temp);
+          const double ce = (2.0 * L0) / (3.0 * KB * dh * Temp);
+          const double T1 = 10.0 + (Temp - 10.0) * exp(-ce * dts);
+          double cf = T1 / Temp;
+          mloss = dmax(mloss, 1.0 - cf);
+          if (cf < 1.0 - ph.cooling_limit) cf = 1.0 - ph.cooling_limit;
+          if (Temp * cf < 10.0) cf = 10.0 / Temp;
+          p[4] = p[4] * cf;
+          const double EK = 0.5 * p[0] * (p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
+          u[4] = EK + ph.cv * p[4];
+        }
+      }
+      P.u[o + 4 * (size_t)BCELLS] = u[4];
+      if (HAS_PAS) P.u[o + (size_t)fp * BCELLS] = u[fp];
+      if (use_prim) {
+        P.prim[o + 4 * (size_t)BCELLS] = p[4];
+        if (HAS_PAS) P.prim[o + (size_t)fp * BCELLS] = p[fp];
+      }
+      if (do_dt) dtl = dmin(dtl, cell_dt<NEQ, MHD>(p, B, ph.gamma));
+    }
+  }
+  if (do_dt) {
+    double v = dtl;
+    for (int s = 16; s > 0; s >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, s));
+    if ((t & 31) == 0) atomic_min_pos(&P.ctl->dtmin_bits, v);
+  }
+  double m = mloss;
+  for (int s = 16; s > 0; s >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, s));
+  if ((t & 31) == 0 && m > 0.0) atomic_max_pos(&P.ctl->maxloss_bits, m);
+}
+
+// ---------------------------------------------------------------------------
+// markByPhysical (amr.f90:142-230).  Physical PRIM from `u`, the one-deep
+// ghost frame from the depth-1 ghost fill of `g` (the state at the start of
+// the last step, which is what the reference's PRIM ghosts hold).
+struct MarkParams {
+  const double* __restrict__ u;
+  const double* __restrict__ g;
+  const DevBlock* __restrict__ blocks;
+  const int32_t* __restrict__ work;
+  int32_t nwork;
+  int32_t* __restrict__ flags;   // per slot
+  int32_t maxlev;
+  double refine_thres, coarse_thres;
+  PhysParams ph;
+};
+
+template <int NEQ, bool MHD>
+__global__ void __launch_bounds__(256) mark_kernel(MarkParams P) {
+  __shared__ double pp[3][18 * 18], pr[3][18 * 18];  // pressure and density, planes k-1..k+1
+  __shared__ int first_refine;                        // first cell (loop order) reaching refineThres
+  __shared__ double bmax;
+  const int t = threadIdx.x;
+  const int i = (t & 15) + 1, j = (t >> 4) + 1;
+  auto q = [](int ii, int jj) { return ii + 18 * jj; };
+  for (int w = blockIdx.x; w < P.nwork; w += gridDim.x) {
+    const int slot = P.work[w];
+    const DevBlock& B = P.blocks[slot];
+    __syncthreads();
+    if (t == 0) { first_refine = 0x7fffffff; bmax = 0.0; }
+    double lmax = 0.0;
+    int lfirst = 0x7fffffff;
+    // plane kk into ring slot kk%3 (kk = 0..17)
+    auto load = [&](int kk) {
+      const int s = kk % 3;
+      double u[NEQ], p[NEQ];
+      get_cell<NEQ>((kk >= 1 && kk <= NC) ? P.u : P.g, B, slot, P.ph.bc, i, j, kk, u);
+      flow2prim<NEQ, MHD>(u, p, P.ph.cv);
+      pp[s][q(i, j)] = p[4];
+      pr[s][q(i, j)] = p[0];
+      if (kk >= 1 && kk <= NC && t < 64) {
+        const int side = t >> 4, r = (t & 15) + 1;
+        int gi, gj;
+        if (side == 0) { gi = 0; gj = r; } else if (side == 1) { gi = NC + 1; gj = r; }
+        else if (side == 2) { gi = r; gj = 0; } else { gi = r; gj = NC + 1; }
+        gather_ghost<NEQ>(P.g, B, slot, P.ph.bc, gi, gj, kk, u);
+        flow2prim<NEQ, MHD>(u, p, P.ph.cv);
+        pp[s][q(gi, gj)] = p[4];
+        pr[s][q(gi, gj)] = p[0];
+      }
+    };
+    load(0);
+    load(1);
+    for (int k = 1; k <= NC; ++k) {
+      load(k + 1);
+      __syncthreads();
+      const int sm = (k - 1) % 3, sc = k % 3, sp = (k + 1) % 3;
+      const double dx2 = 2 * B.dx;
+#pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        double (*a)[18 * 18] = v == 0 ? pp : pr;
+        const double c = a[sc][q(i, j)];
+        const double gx = fabs(a[sc][q(i + 1, j)] - a[sc][q(i - 1, j)]) / c / dx2;
+        const double gy = fabs(a[sc][q(i, j + 1)] - a[sc][q(i, j - 1)]) / c / dx2;
+        const double gz = fabs(a[sp][q(i, j)] - a[sm][q(i, j)]) / c / dx2;
+        const double gr = dmax(dmax(gx, gy), gz);
+        lmax = dmax(lmax, gr);
+        // reference loop order: i outer, j, k inner; pressure before density
+        const int order = (((i - 1) * NC + (j - 1)) * NC + (k - 1)) * 2 + v;
+        if (gr >= P.refine_thres && order < lfirst) lfirst = order;
+      }
+      __syncthreads();
+    }
+    atomicMin(&first_refine, lfirst);
+    for (int s = 16; s > 0; s >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, s));
+    if ((t & 31) == 0) atomic_max_pos(reinterpret_cast<unsigned long long*>(&bmax), lmax);
+    __syncthreads();
+    if (t == 0) {
+      int flag;
+      if (first_refine != 0x7fffffff) flag = (B.level == P.maxlev) ? WX_FLAG_NONE : WX_FLAG_REFINE;
+      else flag = (bmax <= P.coarse_thres && B.level > 1) ? WX_FLAG_COARSE : WX_FLAG_NONE;
+      P.flags[slot] = flag;
+    }
+  }
+}
+
+// refineBlock data copy (amr.f90:355-367): child c (natural order) cell
+// (i,j,k) <- father cell ((n/2)s + (i+1)/2, ...).
+struct Slots8 {
+  int32_t s[8];
+};
+
+__global__ void refine_kernel(double* __restrict__ u, int neq, int father, Slots8 ch) {
+  const int cc = blockIdx.y;
+  const int child = ch.s[cc];
+  const int sx = cc & 1, sy = (cc >> 1) & 1, sz = (cc >> 2) & 1;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < BCELLS * neq; c += gridDim.x * blockDim.x) {
+    const int e = c / BCELLS, r = c % BCELLS;
+    const int i = (r & 15) + 1, j = ((r >> 4) & 15) + 1, k = (r >> 8) + 1;
+    const int ip = 8 * sx + (i + 1) / 2, jp = 8 * sy + (j + 1) / 2, kp = 8 * sz + (k + 1) / 2;
+    u[cell_off(child, neq, e, i, j, k)] = u[cell_off(father, neq, e, ip, jp, kp)];
+  }
+}
+
+// coarseBlocks local branch (amr.f90:1597-1625): father cell <- Fortran SUM
+// of the sibling's 2x2x2 cells (i fastest) / 8.
+__global__ void coarsen_kernel(double* __restrict__ u, int neq, int father, Slots8 ch) {
+  const int sib = blockIdx.y;
+  const int child = ch.s[sib];
+  const int sx = sib & 1, sy = (sib >> 1) & 1, sz = (sib >> 2) & 1;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < 512 * neq; c += gridDim.x * blockDim.x) {
+    const int e = c / 512, r = c % 512;
+    const int i = (r & 7) + 1, j = ((r >> 3) & 7) + 1, k = (r >> 6) + 1;
+    const int i1 = 2 * i - 1, j1 = 2 * j - 1, k1 = 2 * k - 1;
+    double s = 0.0;
+    for (int kk = k1; kk <= k1 + 1; ++kk)
+      for (int jj = j1; jj <= j1 + 1; ++jj)
+        for (int ii = i1; ii <= i1 + 1; ++ii) s += u[cell_off(child, neq, e, ii, jj, kk)];
+    u[cell_off(father, neq, e, i + 8 * sx, j + 8 * sy, k + 8 * sz)] = s / 8.0;
+  }
+}
+
+// Primitive variables of the physical cells (calcPrimsBlock CELLS_PHYS).
+template <int NEQ, bool MHD>
+__global__ void prims_kernel(const double* __restrict__ u, double* __restrict__ prim, const int32_t* __restrict__ work,
+                             int nwork, DevCtl* ctl, double cv) {
+  unsigned pf = 0, df = 0, zd = 0;
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const int slot = work[w];
+    for (int c = threadIdx.x; c < BCELLS; c += blockDim.x) {
+      const size_t o = (size_t)slot * NEQ * BCELLS + c;
+      double uu[NEQ], p[NEQ];
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e) uu[e] = u[o + (size_t)e * BCELLS];
+      const int st = flow2prim<NEQ, MHD>(uu, p, cv);
+      pf += (st == 1); df += (st == 2); zd += (st < 0);
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e) prim[o + (size_t)e * BCELLS] = p[e];
+    }
+  }
+  unsigned m = 0xffffffffu;
+  pf = __reduce_add_sync(m, pf); df = __reduce_add_sync(m, df); zd = __reduce_add_sync(m, zd);
+  if ((threadIdx.x & 31) == 0) {
+    if (pf) atomicAdd(&ctl->cnt[0], (unsigned long long)pf);
+    if (df) atomicAdd(&ctl->cnt[1], (unsigned long long)df);
+    if (zd) atomicAdd(&ctl->cnt[2], (unsigned long long)zd);
+  }
+}
+
+// Fortran U(nbMax, neq, -1:18, -1:18, -1:18) slab at one k (physical k = kf)
+// <-> native [slot][eq][k][j][i].  The slab holds nbMax*neq*20*20 values.
+__global__ void fortran_to_native(const double* __restrict__ slab, double* __restrict__ u, int nbmax, int nslots,
+                                  int neq, int kf) {
+  const long long n = (long long)nslots * neq * PLANE;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int nb = (int)(c % nslots);
+    const long long r = c / nslots;
+    const int e = (int)(r % neq);
+    const int ij = (int)(r / neq);
+    const int i = (ij & 15) + 1, j = (ij >> 4) + 1;
+    u[cell_off(nb, neq, e, i, j, kf)] = slab[nb + (size_t)nbmax * (e + (size_t)neq * ((i + 1) + 20 * (j + 1)))];
+  }
+}
+
+__global__ void native_to_fortran(const double* __restrict__ u, double* __restrict__ slab, int nbmax, int nslots,
+                                  int neq, int kf) {
+  const long long n = (long long)nslots * neq * PLANE;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int nb = (int)(c % nslots);
+    const long long r = c / nslots;
+    const int e = (int)(r % neq);
+    const int ij = (int)(r / neq);
+    const int i = (ij & 15) + 1, j = (ij >> 4) + 1;
+    slab[nb + (size_t)nbmax * (e + (size_t)neq * ((i + 1) + 20 * (j + 1)))] = u[cell_off(nb, neq, e, i, j, kf)];
+  }
+}
+
+}  // namespace wx

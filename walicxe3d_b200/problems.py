@@ -1,0 +1,254 @@
+"""Problem setups (initial conditions and meshes) for the benchmark workloads.
+
+Each builder returns a ``Problem`` with the configuration, the localBlocks
+registry (bID per slot, Morton-ordered) and the conserved variables in the
+native layout ``U[slot][eq][k][j][i]`` (16^3 physical cells per block).
+
+The reference builds its ICs in Fortran user modules; the ones restated
+here are the Sedov-type blast (uniform medium plus a thermal-energy sphere),
+the Brio-Wu shock tube (brio-wu/brio-wu.f90:53-132), the uniform ISM
+(source/uniformISM.f90:87-185), the supernova remnant (source/snr.f90:90-218)
+and spherical winds (source/winds.f90:123-240).  The benchmark meshes are
+synthetic snapshots with the shapes named by the workloads (root grids,
+refinement levels, leaf counts).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import config as C
+from .config import NCELLS, Config
+from .mesh import BlockTree, cell_centres
+
+
+@dataclass
+class Problem:
+    name: str
+    cfg: Config
+    tree: BlockTree
+    local_blocks: np.ndarray      # int32 bID per slot
+    U: np.ndarray                 # float64 [nslots, neq, 16, 16, 16]
+    cooltable: tuple | None = None
+    winds: list = field(default_factory=list)
+    steps: int = 50
+
+    @property
+    def nblocks(self) -> int:
+        return len(self.local_blocks)
+
+    @property
+    def cells(self) -> int:
+        return self.nblocks * NCELLS ** 3
+
+
+def prim2flow(cfg: Config, prim: np.ndarray) -> np.ndarray:
+    """Vectorised prim2flow (source/hydro_core.f90:278-313) over axis 1."""
+    u = np.empty_like(prim)
+    rho = prim[:, 0]
+    u[:, 0] = rho
+    u[:, 1] = rho * prim[:, 1]
+    u[:, 2] = rho * prim[:, 2]
+    u[:, 3] = rho * prim[:, 3]
+    v2 = prim[:, 1] ** 2 + prim[:, 2] ** 2 + prim[:, 3] ** 2
+    u[:, 4] = 0.5 * rho * v2 + cfg.cv * prim[:, 4]
+    if cfg.bfield:
+        if cfg.mhd:
+            u[:, 4] = u[:, 4] + 0.5 * (prim[:, 5] ** 2 + prim[:, 6] ** 2 + prim[:, 7] ** 2)
+        u[:, 5:8] = prim[:, 5:8]
+    if cfg.npassive:
+        u[:, cfg.firstpas:] = prim[:, cfg.firstpas:]
+    return u
+
+
+def _finish(name, cfg, tree, prim_fn, steps, chunk: int = 512, **kw) -> Problem:
+    bids = tree.morton_order()
+    U = np.empty((len(bids), cfg.neqtot, NCELLS, NCELLS, NCELLS))
+    for s in range(0, len(bids), chunk):
+        part = bids[s:s + chunk]
+        xyz = cell_centres(cfg, tree, part)
+        U[s:s + len(part)] = prim2flow(cfg, prim_fn(xyz))
+    return Problem(name, cfg, tree, np.asarray(bids, dtype=np.int32), U, steps=steps, **kw)
+
+
+# ---------------------------------------------------------------------------
+def sedov(nroot: int = 4, steps: int = 50, solver=C.SOLVER_HLLC, limiter=C.LIMITER_MINMOD,
+          radius_cells: float = 3.0, energy: float = 1.0) -> Problem:
+    """Sedov-type blast, adiabatic hydro, single level: nroot^3 root blocks
+    of 16^3 in the unit box, gamma=5/3, ambient rho=1 p=1e-5 v=0, energy E
+    deposited as thermal energy in the cells whose centres lie within
+    radius_cells cells of the box centre; free-flow boundaries."""
+    cfg = Config(solver_type=solver, limiter_type=limiter, nbroot=(nroot,) * 3, maxlev=1,
+                 gamma=5.0 / 3.0, cfl=0.4, visc_eta=5.0e-3)
+    tree = BlockTree(cfg.nbroot, 1).roots()
+    dx = cfg.dx(1)[0]
+
+    # cells whose centres lie inside the sphere: offsets (a+1/2, b+1/2, c+1/2) dx
+    a = np.arange(-int(radius_cells) - 1, int(radius_cells) + 1) + 0.5
+    n_in = int(((a[:, None, None] ** 2 + a[None, :, None] ** 2 + a[None, None, :] ** 2) < radius_cells ** 2).sum())
+
+    def prim_fn(xyz):
+        r = np.sqrt(((xyz - 0.5) ** 2).sum(axis=1))
+        inside = r < radius_cells * dx
+        p = np.full(r.shape, 1.0e-5)
+        p[inside] = (cfg.gamma - 1.0) * energy / (n_in * dx ** 3)
+        prim = np.zeros((xyz.shape[0], cfg.neqtot) + xyz.shape[2:])
+        prim[:, 0] = 1.0
+        prim[:, 4] = p
+        return prim
+
+    return _finish(f"sedov{nroot * NCELLS}", cfg, tree, prim_fn, steps)
+
+
+def brio_wu(nblocks_x: int = 16, steps: int = 0) -> Problem:
+    """Brio-Wu shock tube extruded to 3-D: nblocks_x x 1 x 1 blocks of 16^3,
+    box 1 x 1/16 x 1/16, gamma=2, Bx=0.75, left rho=1 p=1 By=1, right
+    rho=0.125 p=0.1 By=-1 (brio-wu/brio-wu.f90:87-105), HLLD + minmod,
+    CFL 0.4, no viscosity, Powell 8-wave source; the y/z-invariant problem
+    makes free-flow y/z boundaries equivalent to periodic ones."""
+    cfg = Config(bfield=True, mhd=True, solver_type=C.SOLVER_HLLD, limiter_type=C.LIMITER_MINMOD,
+                 eight_wave=True, nbroot=(nblocks_x, 1, 1), maxlev=1, gamma=2.0, cfl=0.4, visc_eta=0.0,
+                 box=(1.0, 1.0 / nblocks_x, 1.0 / nblocks_x), tfin=0.1, dtout=0.01)
+    tree = BlockTree(cfg.nbroot, 1).roots()
+
+    def prim_fn(xyz):
+        x = xyz[:, 0]
+        left = x <= 0.5
+        prim = np.zeros((xyz.shape[0], cfg.neqtot) + xyz.shape[2:])
+        prim[:, 0] = np.where(left, 1.0, 0.125)
+        prim[:, 4] = np.where(left, 1.0, 0.1)
+        prim[:, 5] = 0.75
+        prim[:, 6] = np.where(left, 1.0, -1.0)
+        return prim
+
+    return _finish("brio-wu", cfg, tree, prim_fn, steps or 200)
+
+
+def shock_tube(nblocks: int = 16, axis: int = 0, gamma: float = 1.4, left=(1.0, 0.0, 1.0),
+               right=(0.125, 0.0, 0.1), solver=C.SOLVER_HLLC, limiter=C.LIMITER_MINMOD, eta: float = 0.0,
+               t_end: float = 0.2) -> Problem:
+    """Sod-type shock tube along `axis` (0, 1, 2): nblocks blocks of 16^3 in
+    a box of length 1 along the axis and 1/nblocks across; (rho, u, p) left
+    and right of the mid-plane; free-flow boundaries.  dtout = t_end so the
+    reference's output clipping (hydro_solver.f90:204-207) lands a step
+    exactly on t_end."""
+    nb = [1, 1, 1]
+    nb[axis] = nblocks
+    box = [1.0 / nblocks] * 3
+    box[axis] = 1.0
+    cfg = Config(solver_type=solver, limiter_type=limiter, nbroot=tuple(nb), maxlev=1, gamma=gamma,
+                 visc_eta=eta, box=tuple(box), tfin=t_end, dtout=t_end)
+    tree = BlockTree(cfg.nbroot, 1).roots()
+
+    def prim_fn(xyz):
+        x = xyz[:, axis]
+        lft = x <= 0.5
+        prim = np.zeros((xyz.shape[0], cfg.neqtot) + xyz.shape[2:])
+        prim[:, 0] = np.where(lft, left[0], right[0])
+        prim[:, 1 + axis] = np.where(lft, left[1], right[1])
+        prim[:, 4] = np.where(lft, left[2], right[2])
+        return prim
+
+    return _finish(f"shocktube{axis}", cfg, tree, prim_fn, 0)
+
+
+def blast_amr(nroot: int = 8, maxlev: int = 5, shell_radius: float = 0.1, shell_width: float = 0.004,
+              steps: int = 200, solver=C.SOLVER_HLLC, limiter=C.LIMITER_MINMOD) -> Problem:
+    """Batched AMR blast snapshot: the Sedov setup on nroot^3 root blocks with
+    maxlev levels; the blocks crossing the blast shell (radius shell_radius,
+    half-width shell_width) are refined to maxlev and the face-proximity rule
+    fills the intermediate levels, giving uneven leaf counts per level.  The
+    state is a smooth blast profile: hot rarefied interior, compressed shell
+    moving outwards, cold ambient medium."""
+    cfg = Config(solver_type=solver, limiter_type=limiter, nbroot=(nroot,) * 3, maxlev=maxlev,
+                 gamma=5.0 / 3.0, cfl=0.4, visc_eta=5.0e-3)
+    tree = BlockTree(cfg.nbroot, maxlev).roots()
+    c = np.array([0.5, 0.5, 0.5])
+
+    def crosses(lev, lo, hi):
+        near = np.clip(c, lo, hi)
+        dmin = np.sqrt(((near - c) ** 2).sum())
+        corners = np.array([[lo[0] if a else hi[0], lo[1] if b else hi[1], lo[2] if d else hi[2]]
+                            for a in (0, 1) for b in (0, 1) for d in (0, 1)])
+        dmax = np.sqrt(((corners - c) ** 2).sum(axis=1)).max()
+        return dmin <= shell_radius + shell_width and dmax >= shell_radius - shell_width
+
+    tree.refine_where(crosses, maxlev)
+
+    def prim_fn(xyz):
+        r = np.sqrt(((xyz - c[None, :, None, None, None]) ** 2).sum(axis=1))
+        s = (r - shell_radius) / shell_width
+        shell = np.exp(-s * s)
+        inside = 0.5 * (1.0 - np.tanh(s))
+        prim = np.zeros((xyz.shape[0], cfg.neqtot) + xyz.shape[2:])
+        prim[:, 0] = 1.0 + 3.0 * shell - 0.9 * inside * (1 - shell)
+        prim[:, 4] = 1.0e-5 + 0.5 * inside + 0.8 * shell
+        vr = 0.6 * shell + 0.3 * inside * (r / shell_radius)
+        rr = np.maximum(r, 1e-12)
+        for d in range(3):
+            prim[:, 1 + d] = vr * (xyz[:, d] - c[d]) / rr
+        return prim
+
+    return _finish(f"blast-amr-l{maxlev}", cfg, tree, prim_fn, steps)
+
+
+def cooling_table_synthetic(n: int = 200) -> tuple:
+    """A monotone, smooth Lambda(T) table in loadcooldata format
+    (source/cooling.f90:135-184): n rows of (log10 T, -log10 Lambda) for
+    log T in 4..9, Lambda peaking near 1e5.3 K."""
+    logT = np.linspace(4.0, 9.0, n)
+    logL = -21.6 - 0.9 * (logT - 5.3) ** 2 / (1.0 + 0.35 * np.abs(logT - 5.3)) + 0.25 * np.tanh(logT - 7.5)
+    return logT, -logL
+
+
+def snr_h(nroot: int = 4, maxlev: int = 2, steps: int = 20) -> Problem:
+    """Radiative supernova remnant with hydrogen ionisation (snr/user.f90):
+    uniform ISM n=1 cm^-3, T=1e4 K, neutral fraction 0.99, ejecta 2 Msun and
+    1e51 erg (chi=0.5) inside 1 pc, box 50 pc, EOS_H_RATE + COOL_H, HLLC +
+    minmod, one passive scalar (neutral H density)."""
+    mu0 = 1.3
+    cfg = Config(npassive=1, solver_type=C.SOLVER_HLLC, limiter_type=C.LIMITER_MINMOD,
+                 eos_type=C.EOS_H_RATE, cooling_type=C.COOL_H, nbroot=(nroot,) * 3, maxlev=maxlev,
+                 gamma=5.0 / 3.0, cfl=0.4, visc_eta=5.0e-3, l_sc=C.PC, d_sc=mu0 * C.AMU, v_sc=1.0e5,
+                 box=(50.0 * C.PC,) * 3, tfin=5.0e4 * C.YR, dtout=1.0e4 * C.YR)
+    tree = BlockTree(cfg.nbroot, maxlev).roots()
+    xc = 25.0  # pc, code units
+    rsn = 1.0
+
+    def near(lev, lo, hi):
+        p = np.clip(np.full(3, xc / 50.0), lo, hi)
+        return np.sqrt(((p - xc / 50.0) ** 2).sum()) * 50.0 <= 6.0 * rsn
+
+    tree.refine_where(near, maxlev)
+
+    def prim_fn(xyz):
+        # impose_uniform_ism (uniformISM.f90:124-158)
+        dens_ism = 1.0 * C.AMU * mu0
+        temp_ism, y0 = 1.0e4, 0.99
+        pres_ism = dens_ism / (mu0 * C.AMU) * C.KB * temp_ism
+        prim = np.zeros((xyz.shape[0], cfg.neqtot) + xyz.shape[2:])
+        prim[:, 0] = mu0 * dens_ism / cfg.d_sc
+        prim[:, 4] = pres_ism / cfg.p_sc
+        prim[:, 5] = y0 * dens_ism / cfg.d_sc
+        # detonateSNR (snr.f90:127-206), linear velocity profile
+        msn, esn, chi = 2.0 * C.MSUN, 1.0e51, 0.5
+        R = rsn * C.PC
+        ek, et = chi * esn, (1.0 - chi) * esn
+        dens = msn / (4.0 / 3.0 * C.PI * R ** 3)
+        vmax = np.sqrt(10.0 / 3.0 * ek / msn)
+        pres = (1.0 / cfg.cv) * et / (4.0 / 3.0 * C.PI * R ** 3)
+        pos = xyz * cfg.l_sc
+        d = pos - xc * C.PC
+        dist = np.sqrt((d ** 2).sum(axis=1))
+        m = dist < R
+        vel = np.where(m, dist / R * vmax, 0.0)
+        safe = np.maximum(dist, 1.0)
+        prim[:, 0] = np.where(m, dens / cfg.d_sc, prim[:, 0])
+        for a in range(3):
+            prim[:, 1 + a] = np.where(m, vel * d[:, a] / safe / cfg.v_sc, 0.0)
+        prim[:, 4] = np.where(m, pres / cfg.p_sc, prim[:, 4])
+        prim[:, 5] = np.where(m, 0.0, prim[:, 5])
+        return prim
+
+    return _finish("snr-h", cfg, tree, prim_fn, steps)
