@@ -217,7 +217,11 @@ def main():
 
     prob = build_problem(args.workload)
     w = from_problem(prob)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library runs on it and the timing events are
+    # recorded on it (the default stream's handle 0 would select the
+    # library's own stream)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     w.set_stream(stream.cuda_stream)
     if args.zsplit:
         w.set_zsplit(args.zsplit)

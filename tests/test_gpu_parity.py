@@ -54,11 +54,36 @@ def check(o, g, prob, tol=TOL):
     return err
 
 
-def small_amr(nroot=2, levels=3, solver=C.SOLVER_HLLC, limiter=C.LIMITER_MINMOD):
-    """A balanced multi-level mesh around the box centre."""
-    prob = problems.blast_amr(nroot=nroot, maxlev=levels, shell_radius=0.12, shell_width=0.03, solver=solver,
+def small_amr(nroot=3, levels=3, solver=C.SOLVER_HLLC, limiter=C.LIMITER_MINMOD):
+    """A balanced three-level mesh around the box centre (132 blocks:
+    20 / 48 / 64 per level)."""
+    prob = problems.blast_amr(nroot=nroot, maxlev=levels, shell_radius=0.1, shell_width=0.02, solver=solver,
                               limiter=limiter)
     return prob
+
+
+def inject(father):
+    """refineBlock's copy (amr.f90:355-367) of a [neq,16,16,16] father block
+    into its 8 children, natural order."""
+    out = []
+    for c in range(8):
+        sx, sy, sz = c & 1, (c >> 1) & 1, c >> 2
+        idx = lambda s: 8 * s + (np.arange(16) + 2) // 2 - 1   # 0-based of 8s + (i+1)/2
+        out.append(father[:, idx(sz)][:, :, idx(sy)][:, :, :, idx(sx)])
+    return out
+
+
+def average8(kids):
+    """coarseBlocks' average (amr.f90:1619): Fortran SUM over each 2x2x2
+    section in array order (i fastest), divided by 8."""
+    f = np.empty_like(kids[0])
+    for c, a in enumerate(kids):
+        sx, sy, sz = c & 1, (c >> 1) & 1, c >> 2
+        s = a[:, 0::2, 0::2, 0::2].copy()
+        for (dk, dj, di) in [(0, 0, 1), (0, 1, 0), (0, 1, 1), (1, 0, 0), (1, 0, 1), (1, 1, 0), (1, 1, 1)]:
+            s = s + a[:, dk::2, dj::2, di::2]
+        f[:, 8 * sz:8 * sz + 8, 8 * sy:8 * sy + 8, 8 * sx:8 * sx + 8] = s / 8.0
+    return f
 
 
 def test_sedov_hllc_minmod_50_steps(ncpu):
@@ -68,16 +93,46 @@ def test_sedov_hllc_minmod_50_steps(ncpu):
 
 
 @pytest.mark.parametrize("limiter", [C.LIMITER_NO_AVERAGE, C.LIMITER_NONE, C.LIMITER_MINMOD, C.LIMITER_VANLEER,
-                                     C.LIMITER_ALBADA, C.LIMITER_UMIST, C.LIMITER_WOODWARD, C.LIMITER_SUPERBEE])
+                                     C.LIMITER_UMIST, C.LIMITER_WOODWARD, C.LIMITER_SUPERBEE])
 def test_limiters_hllc(limiter, ncpu):
+    prob = problems.smooth_pulse(2, limiter=limiter)
+    o, g = run_both(prob, 15, ncpu)
+    assert o.counters()[:3] == [0, 0, 0]
+    check(o, g, prob)
+
+
+@pytest.mark.parametrize("limiter", [C.LIMITER_MINMOD, C.LIMITER_VANLEER, C.LIMITER_SUPERBEE])
+def test_limiters_on_strong_blast(limiter, ncpu):
     prob = problems.sedov(2, limiter=limiter)
     o, g = run_both(prob, 15, ncpu)
     check(o, g, prob)
 
 
+def test_albada_limiter_fails_like_the_reference(ncpu):
+    """The reference marks LIMITER_ALBADA "NOT WORKING" (hydro_core.f90:669):
+    its formula is 0/0 where both slopes vanish.  The oracle goes non-finite
+    and the GPU path reports WX_ERR_NAN instead of returning garbage."""
+    from walicxe3d_b200 import WxError
+    prob = problems.smooth_pulse(2, limiter=C.LIMITER_ALBADA)
+    o = oracle.from_problem(prob, threads=ncpu)
+    o.step()
+    assert not np.all(np.isfinite(o.U))
+    g = from_problem(prob)
+    with pytest.raises(WxError) as ei:
+        g.step()
+    assert ei.value.code == 102
+
+
 @pytest.mark.parametrize("solver", [C.SOLVER_HLL, C.SOLVER_HLL1, C.SOLVER_LAX])
 def test_other_hydro_solvers(solver, ncpu):
     prob = problems.sedov(2, solver=solver, limiter=C.LIMITER_VANLEER)
+    o, g = run_both(prob, 15, ncpu)
+    check(o, g, prob)
+
+
+@pytest.mark.parametrize("solver", [C.SOLVER_HLL, C.SOLVER_HLL1, C.SOLVER_LAX, C.SOLVER_HLLC])
+def test_hydro_solvers_smooth(solver, ncpu):
+    prob = problems.smooth_pulse(2, solver=solver, limiter=C.LIMITER_VANLEER)
     o, g = run_both(prob, 15, ncpu)
     check(o, g, prob)
 
@@ -236,18 +291,27 @@ def test_mark_refine_coarsen(ncpu):
     fo = o.mark()[: prob.nblocks]
     fg = g.mark()[: prob.nblocks]
     assert np.array_equal(fo, fg)
+    assert set(np.unique(fg)) <= {0, 1, 2}
     # refine the first level-2 block into 8 free slots, then coarsen back
     lv = [prob.tree.level(int(b)) for b in prob.local_blocks]
     father = lv.index(2)
     kids = list(range(prob.nblocks, prob.nblocks + 8))
-    o.refine(father, kids)
+    n = prob.nblocks + 16
+    Fg, Fo = g.download(n)[father], o.U[father]
     g.refine(father, kids)
-    Uo, Ug = o.U, g.download(prob.nblocks + 16)
-    for s in kids:
-        assert np.array_equal(Ug[s], Uo[s])
-    o.coarsen(kids, father)
+    o.refine(father, kids)
+    Ug, Uo = g.download(n), o.U
+    for c, s in enumerate(kids):
+        assert np.array_equal(Ug[s], inject(Fg)[c])   # device copy = reference copy rule
+        assert np.array_equal(Uo[s], inject(Fo)[c])   # oracle obeys the same rule
+    # perturb the children so the average is not a plain copy back
+    Ug[kids] *= 1.0 + 1e-3 * np.arange(8)[:, None, None, None, None]
+    g.upload(Ug)
     g.coarsen(kids, father)
-    assert np.array_equal(g.download(prob.nblocks + 16)[father], o.U[father])
+    got = g.download(n)[father]
+    assert np.array_equal(got, average8([Ug[s] for s in kids]))
+    o.coarsen(kids, father)
+    assert np.array_equal(o.U[father], average8([Uo[s] for s in kids]))
 
 
 def test_sedov_256_conservation_and_symmetry():

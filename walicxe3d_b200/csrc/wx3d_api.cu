@@ -234,7 +234,9 @@ bool sources_on(const wx_ctx* c) { return c->cfg.eos_type == WX_EOS_H_RATE || c-
 void tick(wx_ctx* c, int kind, bool begin) {
   if (!c->timing || c->timing_mute || c->nev >= 64) return;
   if (begin) c->ev_kind[c->nev / 2] = kind;
-  cudaEventRecord(c->ev[c->nev], c->stream);
+  // external record: inside a stream capture this becomes an event-record
+  // node of the graph, so the replay itself stamps the event
+  cudaEventRecordWithFlags(c->ev[c->nev], c->stream, cudaEventRecordExternal);
   ++c->nev;
 }
 
@@ -514,7 +516,11 @@ int wx3d_set_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb) {
       for (int q = 0; q < 4; ++q) b.fnb[f][q] = -1;
       int y[3] = {x[0], x[1], x[2]};
       y[ax] += side ? 1 : -1;
-      if (y[ax] < 0 || y[ax] >= T.nb[l][ax]) { b.ftype[f] = WX_NEIGH_BOUNDARY; continue; }
+      if (y[ax] < 0 || y[ax] >= T.nb[l][ax]) {
+        b.ftype[f] = WX_NEIGH_BOUNDARY;
+        b.fnb[f][0] = c->cfg.bc[f];
+        continue;
+      }
       const long long nID = T.id(l, y);
       auto it = slot.find(nID);
       if (it != slot.end()) { b.ftype[f] = WX_NEIGH_SAME; b.fnb[f][0] = it->second; continue; }

@@ -30,7 +30,8 @@ struct __align__(16) DevBlock {
   int32_t bc[3];       // block coordinates at its level (bcoords, amr.f90:972)
   int32_t sib[3];      // siblingCoords of this block (amr.f90:831), -1 for roots
   int32_t ftype[6];    // WX_NEIGH_* per face (LEFT..TOP), 0 = empty slot
-  int32_t fnb[6][4];   // neighbour slots: [0] for SAME/COARSER, [0..3] for FINER
+  int32_t fnb[6][4];   // neighbour slots: [0] for SAME/COARSER, [0..3] for FINER;
+                       // for BOUNDARY faces fnb[f][0] holds the BC type
   double dx, dy, dz;   // cell size at this level (init.f90:726-730)
 };
 
@@ -400,70 +401,74 @@ __device__ __forceinline__ void load_cell_rw(const double* a, int slot, int i, i
 }
 
 template <int NEQ>
-__device__ void gather_ghost(const double* __restrict__ a, const DevBlock& b, int slot, const int* bcs, int i, int j,
-                             int k, double* u) {
-  int c[3] = {i, j, k};
-  int f, ax;
-  if (i < 1) { f = 0; ax = 0; }
-  else if (i > NC) { f = 1; ax = 0; }
-  else if (j < 1) { f = 2; ax = 1; }
-  else if (j > NC) { f = 3; ax = 1; }
-  else if (k < 1) { f = 4; ax = 2; }
-  else { f = 5; ax = 2; }
-  const int side = f & 1;
-  const int g = c[ax];
-  const int t1 = (ax == 0) ? 1 : 0;
-  const int t2 = (ax == 2) ? 1 : 2;
+__device__ void gather_ghost(const double* __restrict__ a, const DevBlock& b, int slot, int i, int j, int k,
+                             double* u) {
+  // face and axis of the ghost cell; coordinates are remapped per axis
+  // without local arrays so nothing spills to the stack
+  int f;
+  if (i < 1) f = 0;
+  else if (i > NC) f = 1;
+  else if (j < 1) f = 2;
+  else if (j > NC) f = 3;
+  else if (k < 1) f = 4;
+  else f = 5;
+  const int ax = f >> 1, side = f & 1;
   const int type = b.ftype[f];
   if (type == WX_NEIGH_SAME) {  // boundary.f90:329-366
-    c[ax] = side ? g - NC : g + NC;
-    load_cell<NEQ>(a, b.fnb[f][0], c[0], c[1], c[2], u);
+    const int sh = side ? -NC : NC;
+    if (ax == 0) i += sh; else if (ax == 1) j += sh; else k += sh;
+    load_cell<NEQ>(a, b.fnb[f][0], i, j, k, u);
   } else if (type == WX_NEIGH_COARSER) {  // boundary.f90:385-412
-    c[ax] = side ? 1 : NC;
-    c[t1] = (c[t1] + 1) / 2 + b.sib[t1] * (NC / 2);
-    c[t2] = (c[t2] + 1) / 2 + b.sib[t2] * (NC / 2);
-    load_cell<NEQ>(a, b.fnb[f][0], c[0], c[1], c[2], u);
+    const int fc = side ? 1 : NC;
+    const int ci = ax == 0 ? fc : (i + 1) / 2 + b.sib[0] * (NC / 2);
+    const int cj = ax == 1 ? fc : (j + 1) / 2 + b.sib[1] * (NC / 2);
+    const int ck = ax == 2 ? fc : (k + 1) / 2 + b.sib[2] * (NC / 2);
+    load_cell<NEQ>(a, b.fnb[f][0], ci, cj, ck, u);
   } else if (type == WX_NEIGH_FINER) {  // boundary.f90:494-540
-    const int s1 = (c[t1] - 1) / (NC / 2), s2 = (c[t2] - 1) / (NC / 2);
-    const int src = b.fnb[f][s1 + 2 * s2];
-    int lo[3];
-    lo[ax] = side ? 2 * (g - NC) - 1 : NC + 2 * g - 1;
-    lo[t1] = 2 * (c[t1] - s1 * (NC / 2)) - 1;
-    lo[t2] = 2 * (c[t2] - s2 * (NC / 2)) - 1;
-    const double* p = a + cell_off(src, NEQ, 0, lo[0], lo[1], lo[2]);
+    const int si = (i - 1) / (NC / 2), sj = (j - 1) / (NC / 2), sk = (k - 1) / (NC / 2);
+    // child among the four: transverse sibling bits in x<y<z order
+    const int q = ax == 0 ? sj + 2 * sk : (ax == 1 ? si + 2 * sk : si + 2 * sj);
+    const int src = b.fnb[f][q];
+    auto lo_n = [&](int g) { return side ? 2 * (g - NC) - 1 : NC + 2 * g - 1; };
+    const int li = ax == 0 ? lo_n(i) : 2 * (i - si * (NC / 2)) - 1;
+    const int lj = ax == 1 ? lo_n(j) : 2 * (j - sj * (NC / 2)) - 1;
+    const int lk = ax == 2 ? lo_n(k) : 2 * (k - sk * (NC / 2)) - 1;
+    const double* p = a + cell_off(src, NEQ, 0, li, lj, lk);
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) {
-      const double* q = p + (size_t)e * BCELLS;
+      const double* qq = p + (size_t)e * BCELLS;
       // x outer, y, z inner: the accumulation order of boundary.f90:516-536
       double s = 0.0;
-      s += __ldg(q);
-      s += __ldg(q + PLANE);
-      s += __ldg(q + NC);
-      s += __ldg(q + NC + PLANE);
-      s += __ldg(q + 1);
-      s += __ldg(q + 1 + PLANE);
-      s += __ldg(q + 1 + NC);
-      s += __ldg(q + 1 + NC + PLANE);
+      s += __ldg(qq);
+      s += __ldg(qq + PLANE);
+      s += __ldg(qq + NC);
+      s += __ldg(qq + NC + PLANE);
+      s += __ldg(qq + 1);
+      s += __ldg(qq + 1 + PLANE);
+      s += __ldg(qq + 1 + NC);
+      s += __ldg(qq + 1 + NC + PLANE);
       u[e] = s * 0.125;
     }
-  } else {  // domain boundary, boundary.f90:594-673
-    const int bct = bcs[f];
+  } else {  // domain boundary (boundary.f90:594-673); the BC type sits in fnb[f][0]
+    const int bct = b.fnb[f][0];
+    const int g = ax == 0 ? i : (ax == 1 ? j : k);
+    const int src = bct == WX_BC_REFLECTIVE ? (side ? 2 * NC - g + 1 : 1 - g)
+                                            : (side ? 2 * NC - g + 1 : 1);  // free flow: low copies cell 1
+    if (ax == 0) i = src; else if (ax == 1) j = src; else k = src;
+    load_cell<NEQ>(a, slot, i, j, k, u);
     if (bct == WX_BC_REFLECTIVE) {
-      c[ax] = side ? 2 * NC - g + 1 : 1 - g;
-      load_cell<NEQ>(a, slot, c[0], c[1], c[2], u);
-      u[1 + ax] = -1.0 * u[1 + ax];
-    } else {  // free flow: low faces copy cell 1, high faces mirror
-      c[ax] = side ? 2 * NC - g + 1 : 1;
-      load_cell<NEQ>(a, slot, c[0], c[1], c[2], u);
+      if (ax == 0) u[1] = -1.0 * u[1];
+      else if (ax == 1) u[2] = -1.0 * u[2];
+      else u[3] = -1.0 * u[3];
     }
   }
 }
 
 template <int NEQ>
-__device__ __forceinline__ void get_cell(const double* __restrict__ a, const DevBlock& b, int slot, const int* bcs,
-                                         int i, int j, int k, double* u) {
+__device__ __forceinline__ void get_cell(const double* __restrict__ a, const DevBlock& b, int slot, int i, int j,
+                                         int k, double* u) {
   if (i >= 1 && i <= NC && j >= 1 && j <= NC && k >= 1 && k <= NC) load_cell<NEQ>(a, slot, i, j, k, u);
-  else gather_ghost<NEQ>(a, b, slot, bcs, i, j, k, u);
+  else gather_ghost<NEQ>(a, b, slot, i, j, k, u);
 }
 
 // CFL time step of one cell (hydro_core.f90:503-543, hydro_solver.f90:441-455).

@@ -127,8 +127,8 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel(StageParams P) {
             else { i = r; j = NC + 2 - d; }
           }
           double u[NEQ], p[NEQ];
-          if (inner) get_cell<NEQ>(P.src, B, slot, ph.bc, i, j, kk, u);
-          else gather_ghost<NEQ>(P.src, B, slot, ph.bc, i, j, kk, u);
+          if (inner) get_cell<NEQ>(P.src, B, slot, i, j, kk, u);
+          else gather_ghost<NEQ>(P.src, B, slot, i, j, kk, u);
           const int st = flow2prim<NEQ, MHD>(u, p, ph.cv);
           if (c < PLANE && inner && frame) {
             pf += (st == 1);
@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(256) lax_kernel(LaxParams P) {
       double un[6][NEQ], fl[NEQ], fr[NEQ], pv[NEQ], tmp[NEQ];
       const int di[6] = {1, -1, 0, 0, 0, 0}, dj[6] = {0, 0, 1, -1, 0, 0}, dk[6] = {0, 0, 0, 0, 1, -1};
 #pragma unroll
-      for (int q = 0; q < 6; ++q) get_cell<NEQ>(P.u, B, slot, P.ph.bc, i + di[q], j + dj[q], k + dk[q], un[q]);
+      for (int q = 0; q < 6; ++q) get_cell<NEQ>(P.u, B, slot, i + di[q], j + dj[q], k + dk[q], un[q]);
       double res[NEQ];
 #pragma unroll
       for (int e = 0; e < NEQ; ++e)
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(256) viscous_kernel(ViscParams P) {
 #pragma unroll
       for (int e = 0; e < NEQ; ++e) wm[e] = 0.0;
     } else {
-      gather_ghost<NEQ>(P.up, B, slot, P.ph.bc, i, j, 0, wm);
+      gather_ghost<NEQ>(P.up, B, slot, i, j, 0, wm);
     }
     load_cell_rw<NEQ>(P.w, slot, i, j, 1, wc);
     for (int k = 1; k <= NC; ++k) {
@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(256) viscous_kernel(ViscParams P) {
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) wp[e] = 0.0;
       } else {
-        gather_ghost<NEQ>(P.up, B, slot, P.ph.bc, i, j, NC + 1, wp);
+        gather_ghost<NEQ>(P.up, B, slot, i, j, NC + 1, wp);
       }
       __syncthreads();
 #pragma unroll
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(256) viscous_kernel(ViscParams P) {
 #pragma unroll
           for (int e = 0; e < NEQ; ++e) g[e] = 0.0;
         } else {
-          gather_ghost<NEQ>(P.up, B, slot, P.ph.bc, gi, gj, k, g);
+          gather_ghost<NEQ>(P.up, B, slot, gi, gj, k, g);
         }
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) pl[e][q(gi, gj)] = g[e];

@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(256) mark_kernel(MarkParams P) {
     auto load = [&](int kk) {
       const int s = kk % 3;
       double u[NEQ], p[NEQ];
-      get_cell<NEQ>((kk >= 1 && kk <= NC) ? P.u : P.g, B, slot, P.ph.bc, i, j, kk, u);
+      get_cell<NEQ>((kk >= 1 && kk <= NC) ? P.u : P.g, B, slot, i, j, kk, u);
       flow2prim<NEQ, MHD>(u, p, P.ph.cv);
       pp[s][q(i, j)] = p[4];
       pr[s][q(i, j)] = p[0];
@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(256) mark_kernel(MarkParams P) {
         int gi, gj;
         if (side == 0) { gi = 0; gj = r; } else if (side == 1) { gi = NC + 1; gj = r; }
         else if (side == 2) { gi = r; gj = 0; } else { gi = r; gj = NC + 1; }
-        gather_ghost<NEQ>(P.g, B, slot, P.ph.bc, gi, gj, kk, u);
+        gather_ghost<NEQ>(P.g, B, slot, gi, gj, kk, u);
         flow2prim<NEQ, MHD>(u, p, P.ph.cv);
         pp[s][q(gi, gj)] = p[4];
         pr[s][q(gi, gj)] = p[0];

@@ -125,6 +125,26 @@ def brio_wu(nblocks_x: int = 16, steps: int = 0) -> Problem:
     return _finish("brio-wu", cfg, tree, prim_fn, steps or 200)
 
 
+def smooth_pulse(nroot: int = 2, amplitude: float = 0.2, width: float = 0.15, solver=C.SOLVER_HLLC,
+                 limiter=C.LIMITER_MINMOD) -> Problem:
+    """Smooth Gaussian density/pressure pulse at rest in a uniform medium
+    (rho = p = 1), nroot^3 root blocks: a low-Mach test where no floor or
+    limiter switch is hit, for solver and limiter parity."""
+    cfg = Config(solver_type=solver, limiter_type=limiter, nbroot=(nroot,) * 3, maxlev=1)
+    tree = BlockTree(cfg.nbroot, 1).roots()
+
+    def prim_fn(xyz):
+        r2 = ((xyz - np.array([0.45, 0.5, 0.55])[None, :, None, None, None]) ** 2).sum(axis=1)
+        g = amplitude * np.exp(-r2 / width ** 2)
+        prim = np.zeros((xyz.shape[0], cfg.neqtot) + xyz.shape[2:])
+        prim[:, 0] = 1.0 + g
+        prim[:, 1] = 0.1 * g
+        prim[:, 4] = 1.0 + 1.5 * g
+        return prim
+
+    return _finish("pulse", cfg, tree, prim_fn, 20)
+
+
 def shock_tube(nblocks: int = 16, axis: int = 0, gamma: float = 1.4, left=(1.0, 0.0, 1.0),
                right=(0.125, 0.0, 0.1), solver=C.SOLVER_HLLC, limiter=C.LIMITER_MINMOD, eta: float = 0.0,
                t_end: float = 0.2) -> Problem:
