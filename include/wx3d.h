@@ -238,6 +238,28 @@ int wx3d_kernel_times(wx_ctx* ctx, double* ms4, int32_t* count4);
 int wx3d_get_status(wx_ctx* ctx, wx_status* st);
 int wx3d_reset_status(wx_ctx* ctx);
 
+/* Allocation-free hydro step.  No counterpart in the reference: it exists
+ * for callers that cannot call cudaMalloc -- hosts whose device memory
+ * belongs to their own pool or framework allocator, or that must not grow
+ * their footprint after start-up.  The caller passes the state in its own
+ * device memory: u_in and u_out are [slot][eq][k][j][i] arrays of nslots
+ * blocks that must not overlap, local_blocks is the host-side bID
+ * registry, *state (host) is read and updated like wx3d_step's.  One
+ * main-loop step without source terms is run (it += 1, getTimestep,
+ * Godunov / Lax-Friedrichs, viscous step) on cuda_stream (NULL = default
+ * stream) and the call returns after the stream is synchronised.
+ * Scratch (predictor state, neighbour table, control block) lives in one
+ * fixed device array of the library: nslots x neqtot must not exceed
+ * WX3D_NOALLOC_MAX_BLOCK_EQS (10 MiB of predictor state), otherwise the call
+ * returns WX_ERR_INSUFICIENT_NBMAXPROC.  The first call on each device looks
+ * the array up (cudaGetSymbolAddress) and should come before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race
+ * and must be serialised by the caller.  Source terms (EOS_H_RATE, cooling)
+ * return WX_ERR_UNSUPPORTED. */
+#define WX3D_NOALLOC_MAX_BLOCK_EQS 320
+int wx3d_hydro_step_noalloc(const wx_config* cfg, int32_t nslots, const int32_t* local_blocks,
+                            const double* u_in, double* u_out, wx_state* state, void* cuda_stream);
+
 /* Human-readable text of a status code and of the context's last error. */
 const char* wx3d_error_string(int32_t code);
 int wx3d_last_error(wx_ctx* ctx, char* buf, int32_t len);

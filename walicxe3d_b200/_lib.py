@@ -52,6 +52,8 @@ _SIGNATURES = {
     "wx3d_kernel_times": (ctypes.c_int, [c_void_p, c_double_p, c_int32_p]),
     "wx3d_get_status": (ctypes.c_int, [c_void_p, ctypes.POINTER(WxStatus)]),
     "wx3d_reset_status": (ctypes.c_int, [c_void_p]),
+    "wx3d_hydro_step_noalloc": (ctypes.c_int, [ctypes.POINTER(WxConfig), ctypes.c_int32, c_int32_p, c_void_p,
+                                                c_void_p, ctypes.POINTER(WxState), c_void_p]),
     "wx3d_error_string": (ctypes.c_char_p, [ctypes.c_int32]),
     "wx3d_last_error": (ctypes.c_int, [c_void_p, ctypes.c_char_p, ctypes.c_int32]),
 }

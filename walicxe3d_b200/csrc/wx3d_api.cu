@@ -921,3 +921,254 @@ int wx3d_reset_status(wx_ctx* c) {
 }
 
 }  // extern "C"
+
+// =============================================================================
+// Allocation-free hydro step.
+//
+// Some callers cannot call cudaMalloc: a host whose device memory is owned by
+// its own pool or framework allocator (foreign allocations are forbidden or
+// invisible to its accounting), code that must not grow its footprint after
+// start-up, and embedded drivers that only hand out pointers into buffers
+// they already own.  wx3d_hydro_step_noalloc serves them: the caller passes
+// the input and output state in its own device memory, and everything else
+// the step needs lives in one file-scope device array of fixed size.
+//
+// The scratch holds the predictor state UP of up to WX3D_NOALLOC_MAX_BLOCK_EQS
+// block-equations (blocks x neqtot <= 320, i.e. 10 MiB), the neighbour table,
+// the work list and the step-control block.  Every GPU that loads this
+// library reserves the array until the process exits.  All calls share it
+// and it keeps the last call's contents: the control block (time, dt, CFL
+// minimum, counters) is rewritten from the host at the start of every call,
+// and the predictor stage rewrites every UP cell the later kernels read.
+// Calls whose work overlaps on the GPU (two streams, or two host threads)
+// race on the array and must be serialised by the caller.
+
+namespace {
+
+constexpr int NOALLOC_MAX_BLOCK_EQS = WX3D_NOALLOC_MAX_BLOCK_EQS;
+constexpr int NOALLOC_MAX_BLOCKS = WX3D_NOALLOC_MAX_BLOCK_EQS / 5;  // neqtot >= 5
+constexpr size_t NOALLOC_UP_BYTES = (size_t)NOALLOC_MAX_BLOCK_EQS * BCELLS * sizeof(double);
+constexpr size_t NOALLOC_TABLE_OFF = NOALLOC_UP_BYTES;
+constexpr size_t NOALLOC_WORK_OFF = NOALLOC_TABLE_OFF + ((sizeof(DevBlock) * NOALLOC_MAX_BLOCKS + 255) / 256) * 256;
+constexpr size_t NOALLOC_CTL_OFF = NOALLOC_WORK_OFF + ((4 * NOALLOC_MAX_BLOCKS + 255) / 256) * 256;
+constexpr size_t NOALLOC_BYTES = NOALLOC_CTL_OFF + ((sizeof(DevCtl) + 255) / 256) * 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+// Device address of g_noalloc_scratch per device, looked up once per device
+// with that device current (the symbol is a host-side stand-in in host code).
+constexpr int NOALLOC_MAX_DEVICES = 64;
+unsigned char* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+int noalloc_scratch(int dev, unsigned char** out) {
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return WX_ERR_INVALID_ARG;
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      std::fprintf(stderr, "wx3d_hydro_step_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+      return WX_ERR_CUDA;
+    }
+    g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return WX_OK;
+}
+
+// Neighbour table of one registry (same construction as wx3d_set_mesh, kept
+// separate so that entry point is unchanged).  Fixed-size arrays and a linear
+// bID lookup: at most NOALLOC_MAX_BLOCKS slots, and no heap use.
+int noalloc_find(const int32_t* lb, int n, long long id) {
+  for (int s = 0; s < n; ++s)
+    if (lb[s] == id) return s;
+  return -1;
+}
+
+int noalloc_table(const wx_config& cfg, int n, const int32_t* lb, DevBlock* hb, int32_t* work, int* nwork) {
+  Tree T;
+  T.init(cfg);
+  for (int s = 0; s < n; ++s) {
+    if (lb[s] == -1) continue;
+    if (T.level(lb[s]) < 1 || noalloc_find(lb, s, lb[s]) >= 0) return WX_ERR_MESH;
+  }
+  *nwork = 0;
+  for (int s = 0; s < n; ++s) {
+    hb[s] = DevBlock{};
+    if (lb[s] == -1) continue;
+    DevBlock b{};
+    const long long id = lb[s];
+    const int l = T.level(id);
+    int x[3];
+    T.coords(id, l, x);
+    b.level = l;
+    b.bID = (int32_t)id;
+    for (int d = 0; d < 3; ++d) {
+      b.bc[d] = x[d] + 1;
+      b.sib[d] = l > 1 ? (x[d] & 1) : -1;
+    }
+    const double s2 = std::ldexp(1.0, l - 1);
+    b.dx = cfg.xphystot / ((double)(NC * cfg.nbrootx) * s2) / cfg.l_sc;
+    b.dy = cfg.yphystot / ((double)(NC * cfg.nbrooty) * s2) / cfg.l_sc;
+    b.dz = cfg.zphystot / ((double)(NC * cfg.nbrootz) * s2) / cfg.l_sc;
+    for (int f = 0; f < 6; ++f) {
+      const int ax = f / 2, side = f & 1;
+      for (int q = 0; q < 4; ++q) b.fnb[f][q] = -1;
+      int y[3] = {x[0], x[1], x[2]};
+      y[ax] += side ? 1 : -1;
+      if (y[ax] < 0 || y[ax] >= T.nb[l][ax]) {
+        b.ftype[f] = WX_NEIGH_BOUNDARY;
+        b.fnb[f][0] = cfg.bc[f];
+        continue;
+      }
+      int ns = noalloc_find(lb, n, T.id(l, y));
+      if (ns >= 0) { b.ftype[f] = WX_NEIGH_SAME; b.fnb[f][0] = ns; continue; }
+      if (l > 1) {
+        int z[3] = {y[0] / 2, y[1] / 2, y[2] / 2};
+        ns = noalloc_find(lb, n, T.id(l - 1, z));
+        if (ns >= 0) { b.ftype[f] = WX_NEIGH_COARSER; b.fnb[f][0] = ns; continue; }
+      }
+      if (l >= T.maxlev) return WX_ERR_MESH;
+      const int t1 = ax == 0 ? 1 : 0, t2 = ax == 2 ? 1 : 2;
+      b.ftype[f] = WX_NEIGH_FINER;
+      for (int q = 0; q < 4; ++q) {
+        int ch[3];
+        ch[ax] = 2 * y[ax] + (side ? 0 : 1);
+        ch[t1] = 2 * y[t1] + (q & 1);
+        ch[t2] = 2 * y[t2] + (q >> 1);
+        ns = noalloc_find(lb, n, T.id(l + 1, ch));
+        if (ns < 0) return WX_ERR_MESH;
+        b.fnb[f][q] = ns;
+      }
+    }
+    hb[s] = b;
+    work[(*nwork)++] = s;
+  }
+  return WX_OK;
+}
+
+// Physical parameters of a bare config (as fill_phys does for a context).
+void noalloc_phys(const wx_config& f, PhysParams& p) {
+  p.gamma = f.gamma;
+  p.cv = 1.0 / (f.gamma - 1.0);
+  p.cfl = f.cfl;
+  p.eta = f.visc_eta;
+  p.mu0 = f.mu0; p.mui = f.mui; p.ion_thres = f.ion_thres;
+  p.d_sc = f.d_sc;
+  p.p_sc = f.d_sc * (f.v_sc * f.v_sc);
+  p.e_sc = p.p_sc;
+  p.t_sc = f.l_sc / f.v_sc;
+  p.dtout = f.dtout;
+  p.cooling_limit = f.cooling_limit;
+  p.limiter = f.limiter_type;
+  p.eight_wave = f.eight_wave;
+  for (int i = 0; i < 6; ++i) p.bc[i] = f.bc[i];
+  p.eos = f.eos_type;
+  p.cooling = f.cooling_type;
+  p.fp = 5 + 3 * (f.bfield ? 1 : 0);
+  p.npassive = f.npassive;
+}
+
+int noalloc_grid(const void* fn, int threads, size_t smem, int items, int nsm) {
+  int per = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, smem);
+  per = std::max(per, 1);
+  return std::max(1, std::min(items, per * nsm));
+}
+
+}  // namespace
+
+extern "C" int wx3d_hydro_step_noalloc(const wx_config* cfg, int32_t nslots, const int32_t* local_blocks,
+                                       const double* u_in, double* u_out, wx_state* state, void* cuda_stream) {
+  if (!cfg || !local_blocks || !u_in || !u_out || !state || nslots <= 0) return WX_ERR_INVALID_ARG;
+  std::string why;
+  int rc = validate(*cfg, why);
+  if (rc) { std::fprintf(stderr, "wx3d_hydro_step_noalloc: %s\n", why.c_str()); return rc; }
+  if (cfg->eos_type == WX_EOS_H_RATE || cfg->cooling_type != WX_COOL_NONE) {
+    std::fprintf(stderr, "wx3d_hydro_step_noalloc: source terms are not part of the allocation-free step\n");
+    return WX_ERR_UNSUPPORTED;
+  }
+  if ((long long)nslots * cfg->neqtot > NOALLOC_MAX_BLOCK_EQS || nslots > NOALLOC_MAX_BLOCKS) {
+    std::fprintf(stderr,
+                 "wx3d_hydro_step_noalloc: %d slots x %d equations exceeds the fixed scratch of %d block-equations "
+                 "(%d blocks); use wx3d_init/wx3d_step for larger meshes\n",
+                 nslots, cfg->neqtot, NOALLOC_MAX_BLOCK_EQS, NOALLOC_MAX_BLOCKS);
+    return WX_ERR_INSUFICIENT_NBMAXPROC;
+  }
+  Kern k;
+  if (!select_kern(*cfg, k)) return WX_ERR_UNSUPPORTED;
+  int dev = 0, nsm = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess) return WX_ERR_NO_DEVICE;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  unsigned char* base = nullptr;
+  if ((rc = noalloc_scratch(dev, &base))) return rc;
+  double* dUP = reinterpret_cast<double*>(base);
+  DevBlock* dBlocks = reinterpret_cast<DevBlock*>(base + NOALLOC_TABLE_OFF);
+  int32_t* dWork = reinterpret_cast<int32_t*>(base + NOALLOC_WORK_OFF);
+  DevCtl* dCtl = reinterpret_cast<DevCtl*>(base + NOALLOC_CTL_OFF);
+
+  DevBlock hb[NOALLOC_MAX_BLOCKS];
+  int32_t work[NOALLOC_MAX_BLOCKS];
+  int nwork = 0;
+  if ((rc = noalloc_table(*cfg, nslots, local_blocks, hb, work, &nwork))) {
+    std::fprintf(stderr, "wx3d_hydro_step_noalloc: invalid mesh\n");
+    return rc;
+  }
+  if (nwork == 0) return WX_ERR_MESH;
+  int zsplit = 1;
+  while (zsplit < 8 && nwork * zsplit < 2 * nsm) zsplit *= 2;
+
+  PhysParams ph{};
+  noalloc_phys(*cfg, ph);
+  DevCtl h{};
+  h.time = state->time;
+  h.dt = state->dt;
+  h.it = state->it;
+  h.nextout = state->nextout;
+  h.dumpout = state->dumpout;
+  const double big = 1.0e30;
+  std::memcpy(&h.dtmin_bits, &big, 8);
+
+  cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
+  auto ck = [](cudaError_t e) { return e == cudaSuccess ? WX_OK : WX_ERR_CUDA; };
+  if ((rc = ck(cudaFuncSetAttribute(k.stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem)))) return rc;
+  if ((rc = ck(cudaFuncSetAttribute(k.stage2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem)))) return rc;
+  if ((rc = ck(cudaMemcpyAsync(dBlocks, hb, sizeof(DevBlock) * nslots, cudaMemcpyHostToDevice, s)))) return rc;
+  if ((rc = ck(cudaMemcpyAsync(dWork, work, 4 * (size_t)nwork, cudaMemcpyHostToDevice, s)))) return rc;
+  if ((rc = ck(cudaMemcpyAsync(dCtl, &h, sizeof(DevCtl), cudaMemcpyHostToDevice, s)))) return rc;
+
+  // getTimestep on u_in, then the step sequence of enqueue_solver
+  DtParams D{u_in, dBlocks, dWork, nwork, dCtl, ph};
+  k.dt<<<noalloc_grid((const void*)k.dt, 256, 0, nwork, nsm), 256, 0, s>>>(D);
+  step_begin_kernel<<<1, 1, 0, s>>>(dCtl, ph.cfl, 0, ph.dtout, ph.t_sc, 1);
+  const int solver = cfg->solver_type;
+  int zero_ghost = 0;
+  auto stage = [&](void (*fn)(StageParams), const double* src, double* out, double factor) {
+    StageParams P{src, u_in, out, dBlocks, dWork, nwork * zsplit, zsplit, dCtl, factor, ph};
+    fn<<<noalloc_grid((const void*)fn, STAGE_THREADS, k.smem, nwork * zsplit, nsm), STAGE_THREADS, k.smem, s>>>(P);
+  };
+  if (solver == WX_SOLVER_LAX) {
+    LaxParams L{u_in, u_out, dBlocks, dWork, nwork, dCtl, ph};
+    k.lax<<<noalloc_grid((const void*)k.lax, 256, 0, nwork, nsm), 256, 0, s>>>(L);
+    zero_ghost = 1;
+  } else if (solver == WX_SOLVER_HLL1) {
+    stage(k.stage1, u_in, u_out, 1.0);
+    zero_ghost = 1;
+  } else {
+    stage(k.stage1, u_in, dUP, 0.5);
+    stage(k.stage2, dUP, u_out, 1.0);
+  }
+  ViscParams V{u_out, dUP, dBlocks, dWork, nwork, zero_ghost, 1, dCtl, ph};
+  k.visc<<<noalloc_grid((const void*)k.visc, 256, 0, nwork, nsm), 256, 0, s>>>(V);
+  step_end_kernel<<<1, 1, 0, s>>>(dCtl, 1);
+  if ((rc = ck(cudaGetLastError()))) return rc;
+  if ((rc = ck(cudaMemcpyAsync(&h, dCtl, sizeof(DevCtl), cudaMemcpyDeviceToHost, s)))) return rc;
+  if ((rc = ck(cudaStreamSynchronize(s)))) return rc;
+  state->time = h.time;
+  state->dt = h.dt;
+  state->it = h.it;
+  state->nextout = h.nextout;
+  state->dumpout = h.dumps != 0;
+  if (h.cnt[2]) return WX_ERR_DIVISION_BY_ZERO;
+  if (h.cnt[3]) return WX_ERR_NAN;
+  return WX_OK;
+}
