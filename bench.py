@@ -77,7 +77,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
@@ -223,8 +223,12 @@ def main():
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     w.set_stream(stream.cuda_stream)
+    tuned = None
     if args.zsplit:
         w.set_zsplit(args.zsplit)
+    else:
+        from walicxe3d_b200.autotune import tune
+        tuned = tune(w, prob, cache=None, reps=2)
     w.set_timing(True)
 
     # --- warm-up (graph capture happens here) ---
@@ -315,7 +319,8 @@ def main():
                        "levels": sorted({int(prob.tree.level(int(b))) for b in prob.local_blocks}),
                        "l2": "state arrays larger than L2 (%.2f GB each)" % (state_bytes / 1e9),
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       "path": "wx3d_run: CUDA graph of 2 steps replayed"},
+                       "path": "wx3d_run: CUDA graph of 2 steps replayed",
+                       "autotune": tuned and {"zsplit": tuned["zsplit"], "ms_per_pass": tuned["ms_per_pass"]}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "kernel": "stage_kernel<ORDER=2> (corrector)", "peak_source": peak_src,

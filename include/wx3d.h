@@ -167,6 +167,13 @@ int wx3d_get_neighbours(wx_ctx* ctx, int32_t nslots, int32_t* face_type, int32_t
  * wx3d_set_mesh picks a default; the autotuner overrides it. */
 int wx3d_set_zsplit(wx_ctx* ctx, int32_t zsplit);
 
+/* Autotuner of the stage launch shape for the current mesh: times the
+ * predictor and corrector stages (reps passes each) for z-slab splits
+ * 1, 2, 4, 8 -- on the live state, without changing it -- and keeps the
+ * fastest.  ms4 (may be NULL) receives the time per pass of each split,
+ * *best (may be NULL) the chosen split. */
+int wx3d_autotune(wx_ctx* ctx, int32_t reps, double* ms4, int32_t* best);
+
 /* Conserved variables, native layout: u[slot][eq][k][j][i], 16^3 physical
  * cells per block, host memory (pinned or pageable). */
 int wx3d_upload_blocks(wx_ctx* ctx, int32_t nslots, const double* u);

@@ -1,0 +1,45 @@
+"""Autotuner of the stage launch shape, with an on-disk cache.
+
+The stage kernels run one CTA per (block, z-slab).  How many slabs a block
+is cut into trades parallelism (small meshes leave SMs idle) against
+redundant halo planes (each slab reloads two planes on either side).  The
+best split depends on the block count, the levels and the equation set, so
+it is measured on the live mesh (wx3d_autotune) and cached by a workload
+signature in a JSON file.
+"""
+from __future__ import annotations
+
+import json
+import os
+from pathlib import Path
+
+DEFAULT_CACHE = Path(os.environ.get("WX3D_TUNE_CACHE", Path.home() / ".cache" / "wx3d" / "tuning.json"))
+
+
+def signature(cfg, nblocks: int, levels) -> str:
+    lv = ",".join(str(int(l)) for l in sorted(set(levels)))
+    return f"neq{cfg.neqtot}-s{cfg.solver_type}-l{cfg.limiter_type}-mhd{int(cfg.mhd)}-nb{nblocks}-lev{lv}"
+
+
+def tune(w, prob, cache: Path | None = DEFAULT_CACHE, reps: int = 3, force: bool = False) -> dict:
+    """Picks the z-slab split for w's mesh; returns a record of the choice."""
+    levels = [prob.tree.level(int(b)) for b in prob.local_blocks]
+    key = signature(prob.cfg, prob.nblocks, levels)
+    table = {}
+    if cache is not None and cache.exists():
+        try:
+            table = json.loads(cache.read_text())
+        except ValueError:
+            table = {}
+    if key in table and not force:
+        w.set_zsplit(int(table[key]["zsplit"]))
+        return dict(table[key], cached=True, key=key)
+    best, ms = w.autotune(reps)
+    rec = {"zsplit": best, "ms_per_pass": {str(k): v for k, v in ms.items()}}
+    if cache is not None:
+        cache.parent.mkdir(parents=True, exist_ok=True)
+        table[key] = rec
+        tmp = cache.with_suffix(".tmp")
+        tmp.write_text(json.dumps(table, indent=1, sort_keys=True))
+        tmp.replace(cache)
+    return dict(rec, cached=False, key=key)

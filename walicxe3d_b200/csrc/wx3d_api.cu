@@ -35,22 +35,36 @@ struct Kern {
   void (*src)(SrcParams) = nullptr;
   void (*mark)(MarkParams) = nullptr;
   void (*prims)(const double*, double*, const int32_t*, int, DevCtl*, double) = nullptr;
-  size_t smem = 0;
+  size_t smem1 = 0;  // dynamic shared memory of the predictor and the corrector
+  size_t smem2 = 0;
 };
 
-template <int NEQ, bool MHD, int SOLVER>
+template <int NEQ, bool MHD, int SOLVER, int LIM>
 Kern make_kern() {
   Kern k;
-  k.stage1 = stage_kernel<NEQ, MHD, SOLVER, 1>;
-  k.stage2 = stage_kernel<NEQ, MHD, SOLVER, 2>;
+  k.stage1 = stage_kernel<NEQ, MHD, SOLVER, 1, LIM_RUNTIME>;
+  k.stage2 = stage_kernel<NEQ, MHD, SOLVER, 2, LIM>;
   k.lax = lax_kernel<NEQ, MHD>;
   k.visc = viscous_kernel<NEQ, MHD>;
   k.dt = dt_kernel<NEQ, MHD>;
   k.src = source_kernel<NEQ, MHD>;
   k.mark = mark_kernel<NEQ, MHD>;
   k.prims = prims_kernel<NEQ, MHD>;
-  k.smem = stage_smem_bytes<NEQ>();
+  k.smem1 = stage_smem_bytes<NEQ, MHD, 1>();
+  k.smem2 = stage_smem_bytes<NEQ, MHD, 2>();
   return k;
+}
+
+// Limiters compiled into the corrector for the common cases; the others use
+// the run-time switch.
+template <int NEQ, bool MHD, int SOLVER>
+Kern make_kern_lim(int lim) {
+  if constexpr (NEQ == 5) {
+    if (lim == WX_LIMITER_VANLEER) return make_kern<NEQ, MHD, SOLVER, WX_LIMITER_VANLEER>();
+    if (lim == WX_LIMITER_SUPERBEE) return make_kern<NEQ, MHD, SOLVER, WX_LIMITER_SUPERBEE>();
+  }
+  if (lim == WX_LIMITER_MINMOD) return make_kern<NEQ, MHD, SOLVER, WX_LIMITER_MINMOD>();
+  return make_kern<NEQ, MHD, SOLVER, LIM_RUNTIME>();
 }
 
 // Supported combinations: hydro with 0..2 passives (HLL/HLL1/HLLC/LAX) and
@@ -59,21 +73,22 @@ bool select_kern(const wx_config& c, Kern& k) {
   const bool mhd = c.bfield != 0;
   const int s = c.solver_type;
   const int rs = (s == WX_SOLVER_HLL1 || s == WX_SOLVER_LAX) ? WX_SOLVER_HLL : s;
+  const int lim = c.limiter_type;
   if (!mhd) {
     if (rs != WX_SOLVER_HLL && rs != WX_SOLVER_HLLC) return false;
     const bool c_ = rs == WX_SOLVER_HLLC;
     switch (c.neqtot) {
-      case 5: k = c_ ? make_kern<5, false, WX_SOLVER_HLLC>() : make_kern<5, false, WX_SOLVER_HLL>(); return true;
-      case 6: k = c_ ? make_kern<6, false, WX_SOLVER_HLLC>() : make_kern<6, false, WX_SOLVER_HLL>(); return true;
-      case 7: k = c_ ? make_kern<7, false, WX_SOLVER_HLLC>() : make_kern<7, false, WX_SOLVER_HLL>(); return true;
+      case 5: k = c_ ? make_kern_lim<5, false, WX_SOLVER_HLLC>(lim) : make_kern_lim<5, false, WX_SOLVER_HLL>(lim); return true;
+      case 6: k = c_ ? make_kern_lim<6, false, WX_SOLVER_HLLC>(lim) : make_kern_lim<6, false, WX_SOLVER_HLL>(lim); return true;
+      case 7: k = c_ ? make_kern_lim<7, false, WX_SOLVER_HLLC>(lim) : make_kern_lim<7, false, WX_SOLVER_HLL>(lim); return true;
       default: return false;
     }
   }
   if (c.neqtot != 8) return false;
   switch (rs) {
-    case WX_SOLVER_HLL: k = make_kern<8, true, WX_SOLVER_HLL>(); return true;
-    case WX_SOLVER_HLLE: k = make_kern<8, true, WX_SOLVER_HLLE>(); return true;
-    case WX_SOLVER_HLLD: k = make_kern<8, true, WX_SOLVER_HLLD>(); return true;
+    case WX_SOLVER_HLL: k = make_kern<8, true, WX_SOLVER_HLL, LIM_RUNTIME>(); return true;
+    case WX_SOLVER_HLLE: k = make_kern<8, true, WX_SOLVER_HLLE, LIM_RUNTIME>(); return true;
+    case WX_SOLVER_HLLD: k = make_kern<8, true, WX_SOLVER_HLLD, LIM_RUNTIME>(); return true;
     default: return false;
   }
 }
@@ -248,8 +263,8 @@ int grid_for(wx_ctx* c, const void* fn, int threads, size_t smem, int items) {
 }
 
 int set_stage_attrs(wx_ctx* c) {
-  WX_CUDA(cudaFuncSetAttribute(c->k.stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->k.smem));
-  WX_CUDA(cudaFuncSetAttribute(c->k.stage2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->k.smem));
+  WX_CUDA(cudaFuncSetAttribute(c->k.stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->k.smem1));
+  WX_CUDA(cudaFuncSetAttribute(c->k.stage2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->k.smem2));
   return WX_OK;
 }
 
@@ -267,10 +282,11 @@ int launch_dt(wx_ctx* c, const double* u) {
 int launch_stage(wx_ctx* c, int order, const double* src, const double* base, double* out, double factor) {
   StageParams P{src, base, out, c->dBlocks, c->dWork, c->nwork * c->zsplit, c->zsplit, c->dCtl, factor, c->ph};
   auto fn = order == 1 ? c->k.stage1 : c->k.stage2;
-  const int grid = grid_for(c, (const void*)fn, STAGE_THREADS, c->k.smem, c->nwork * c->zsplit);
+  const size_t smem = order == 1 ? c->k.smem1 : c->k.smem2;
+  const int grid = grid_for(c, (const void*)fn, STAGE_THREADS, smem, c->nwork * c->zsplit);
   const int kind = (order == 2 || factor == 1.0) ? 1 : 0;
   tick(c, kind, true);
-  fn<<<grid, STAGE_THREADS, c->k.smem, c->stream>>>(P);
+  fn<<<grid, STAGE_THREADS, smem, c->stream>>>(P);
   WX_LAUNCHED();
   tick(c, kind, false);
   return WX_OK;
@@ -569,6 +585,56 @@ int wx3d_set_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb) {
 int wx3d_set_zsplit(wx_ctx* c, int32_t zsplit) {
   if (!c || (zsplit != 1 && zsplit != 2 && zsplit != 4 && zsplit != 8)) return WX_ERR_INVALID_ARG;
   c->zsplit = zsplit;
+  invalidate_graph(c);
+  return WX_OK;
+}
+
+// Measured choice of the z-slab split: times the predictor and corrector
+// stages (which write only the UP and W scratch arrays, so U and the
+// simulation state are untouched) for every split and keeps the fastest.
+int wx3d_autotune(wx_ctx* c, int32_t reps, double* ms4, int32_t* best) {
+  if (!ready(c) || reps <= 0) return WX_ERR_INVALID_ARG;
+  if (c->cfg.solver_type == WX_SOLVER_LAX) {
+    if (best) *best = 1;
+    return WX_OK;
+  }
+  int rc;
+  if (!c->dt_valid) {
+    if ((rc = launch_dt(c, c->dU))) return rc;
+    c->dt_valid = true;
+  }
+  cudaEvent_t e0, e1;
+  WX_CUDA(cudaEventCreate(&e0));
+  WX_CUDA(cudaEventCreate(&e1));
+  const bool timing = c->timing;
+  c->timing = false;
+  const int splits[4] = {1, 2, 4, 8};
+  double bestms = 1e300;
+  int bz = c->zsplit;
+  for (int s = 0; s < 4; ++s) {
+    c->zsplit = splits[s];
+    // one untimed pass, then reps timed passes of both stages
+    for (int r = 0; r <= reps; ++r) {
+      if (r == 1) cudaEventRecord(e0, c->stream);
+      if ((rc = launch_stage(c, 1, c->dU, c->dU, c->dUP, 0.5))) { c->timing = timing; return rc; }
+      if (c->cfg.solver_type != WX_SOLVER_HLL1 && (rc = launch_stage(c, 2, c->dUP, c->dU, c->dW, 1.0))) {
+        c->timing = timing;
+        return rc;
+      }
+    }
+    cudaEventRecord(e1, c->stream);
+    WX_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    WX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    const double per = ms / reps;
+    if (ms4) ms4[s] = per;
+    if (per < bestms) { bestms = per; bz = splits[s]; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->timing = timing;
+  c->zsplit = bz;
+  if (best) *best = bz;
   invalidate_graph(c);
   return WX_OK;
 }
@@ -1130,8 +1196,8 @@ extern "C" int wx3d_hydro_step_noalloc(const wx_config* cfg, int32_t nslots, con
 
   cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
   auto ck = [](cudaError_t e) { return e == cudaSuccess ? WX_OK : WX_ERR_CUDA; };
-  if ((rc = ck(cudaFuncSetAttribute(k.stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem)))) return rc;
-  if ((rc = ck(cudaFuncSetAttribute(k.stage2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem)))) return rc;
+  if ((rc = ck(cudaFuncSetAttribute(k.stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem1)))) return rc;
+  if ((rc = ck(cudaFuncSetAttribute(k.stage2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem2)))) return rc;
   if ((rc = ck(cudaMemcpyAsync(dBlocks, hb, sizeof(DevBlock) * nslots, cudaMemcpyHostToDevice, s)))) return rc;
   if ((rc = ck(cudaMemcpyAsync(dWork, work, 4 * (size_t)nwork, cudaMemcpyHostToDevice, s)))) return rc;
   if ((rc = ck(cudaMemcpyAsync(dCtl, &h, sizeof(DevCtl), cudaMemcpyHostToDevice, s)))) return rc;
@@ -1142,20 +1208,20 @@ extern "C" int wx3d_hydro_step_noalloc(const wx_config* cfg, int32_t nslots, con
   step_begin_kernel<<<1, 1, 0, s>>>(dCtl, ph.cfl, 0, ph.dtout, ph.t_sc, 1);
   const int solver = cfg->solver_type;
   int zero_ghost = 0;
-  auto stage = [&](void (*fn)(StageParams), const double* src, double* out, double factor) {
+  auto stage = [&](void (*fn)(StageParams), size_t smem, const double* src, double* out, double factor) {
     StageParams P{src, u_in, out, dBlocks, dWork, nwork * zsplit, zsplit, dCtl, factor, ph};
-    fn<<<noalloc_grid((const void*)fn, STAGE_THREADS, k.smem, nwork * zsplit, nsm), STAGE_THREADS, k.smem, s>>>(P);
+    fn<<<noalloc_grid((const void*)fn, STAGE_THREADS, smem, nwork * zsplit, nsm), STAGE_THREADS, smem, s>>>(P);
   };
   if (solver == WX_SOLVER_LAX) {
     LaxParams L{u_in, u_out, dBlocks, dWork, nwork, dCtl, ph};
     k.lax<<<noalloc_grid((const void*)k.lax, 256, 0, nwork, nsm), 256, 0, s>>>(L);
     zero_ghost = 1;
   } else if (solver == WX_SOLVER_HLL1) {
-    stage(k.stage1, u_in, u_out, 1.0);
+    stage(k.stage1, k.smem1, u_in, u_out, 1.0);
     zero_ghost = 1;
   } else {
-    stage(k.stage1, u_in, dUP, 0.5);
-    stage(k.stage2, dUP, u_out, 1.0);
+    stage(k.stage1, k.smem1, u_in, dUP, 0.5);
+    stage(k.stage2, k.smem2, dUP, u_out, 1.0);
   }
   ViscParams V{u_out, dUP, dBlocks, dWork, nwork, zero_ghost, 1, dCtl, ph};
   k.visc<<<noalloc_grid((const void*)k.visc, 256, 0, nwork, nsm), 256, 0, s>>>(V);

@@ -88,10 +88,11 @@ __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : 
 // flow2prim (hydro_core.f90:323-378).  Returns istat: 0 ok, 1 pressure
 // floor, 2 density floor, -1 zero density.
 template <int NEQ, bool MHD>
-__device__ __forceinline__ int flow2prim(const double* u, double* p, double cv) {
+__device__ __forceinline__ int flow2prim(const double* u, double* p, double cv, double* rinv_out = nullptr) {
   int istat = 0;
   if (u[0] == 0.0) istat = -1;
   const double rinv = 1.0 / u[0];
+  if (rinv_out) *rinv_out = rinv;
   p[0] = u[0];
   p[1] = u[1] * rinv;
   p[2] = u[2] * rinv;
@@ -100,7 +101,11 @@ __device__ __forceinline__ int flow2prim(const double* u, double* p, double cv) 
   if (MHD) pr = pr - 0.5 * (u[5] * u[5] + u[6] * u[6] + u[7] * u[7]) / cv;
   if (pr < 1.0e-30) { pr = 1.0e-30; if (istat == 0) istat = 1; }
   p[4] = pr;
-  if (p[0] < 1.0e-40) { p[0] = 1.0e-40; if (istat >= 0) istat = 2; }
+  if (p[0] < 1.0e-40) {
+    p[0] = 1.0e-40;
+    if (istat >= 0) istat = 2;
+    if (rinv_out) *rinv_out = 1.0e40;
+  }
 #pragma unroll
   for (int e = 5; e < NEQ; ++e) p[e] = u[e];
   return istat;
@@ -179,8 +184,87 @@ __device__ __forceinline__ double average(double a, double b, int opt) {
   }
 }
 
+// average with the limiter fixed at compile time; LIM_RUNTIME dispatches on
+// the run-time value instead.
+constexpr int LIM_RUNTIME = -100;
+
+template <int LIM>
+__device__ __forceinline__ double average_t(double a, double b, int opt) {
+  if constexpr (LIM == WX_LIMITER_MINMOD) {
+    const double s = copysign(1.0, a);
+    return s * dmax(0.0, dmin(fabs(a), s * b));
+  } else if constexpr (LIM == WX_LIMITER_VANLEER) {
+    const double ab = a * b;
+    return (ab <= 0.0) ? 0.0 : ab * (a + b) / (a * a + b * b);
+  } else if constexpr (LIM == WX_LIMITER_SUPERBEE) {
+    const double s = copysign(1.0, b);
+    const double c = dmin(2.0 * fabs(b), s * a);
+    const double d = dmin(fabs(b), 2.0 * s * a);
+    return s * dmax(dmax(0.0, c), d);
+  } else {
+    return average(a, b, opt);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Riemann solvers along x of permuted primitive states.
+
+// HLL with the sound speeds supplied by the caller (hll.f90:175-260).
+template <int NEQ>
+__device__ __forceinline__ void riemann_hll_c(const double* pL, const double* pR, double cl, double cr, double* f,
+                                              double cv) {
+  const double sl = dmin(pL[1] - cl, pR[1] - cr);
+  const double sr = dmax(pL[1] + cl, pR[1] + cr);
+  if (sl >= 0.0) { xflux<NEQ, false>(pL, f, cv); return; }
+  if (sr <= 0.0) { xflux<NEQ, false>(pR, f, cv); return; }
+  double fL[NEQ], fR[NEQ], uL[NEQ], uR[NEQ];
+  xflux<NEQ, false>(pL, fL, cv);
+  xflux<NEQ, false>(pR, fR, cv);
+  prim2flow<NEQ, false>(pL, uL, cv);
+  prim2flow<NEQ, false>(pR, uR, cv);
+  const double inv = 1.0 / (sr - sl);
+  const double slsr = sl * sr;
+#pragma unroll
+  for (int e = 0; e < NEQ; ++e) f[e] = (sr * fL[e] - sl * fR[e] + slsr * (uR[e] - uL[e])) * inv;
+}
+
+// HLLC with sound speeds and 1/rho supplied by the caller (hllc.f90:209-357).
+// The star state needs 1/(sk-sst) and 1/(sk-u_k); both come from one
+// reciprocal of their product.
+template <int NEQ>
+__device__ __forceinline__ void riemann_hllc_c(const double* pL, const double* pR, double cl, double cr, double rl,
+                                               double rr, double* f, double cv) {
+  const double dl = pL[0], dr = pR[0], ul = pL[1], ur = pR[1];
+  const double sl = dmin(ul - cl, ur - cr);
+  const double sr = dmax(ul + cl, ur + cr);
+  const double sst = (pR[4] - pL[4] + dl * ul * (sl - ul) - dr * ur * (sr - ur)) / (dl * (sl - ul) - dr * (sr - ur));
+  const bool useL = (sl > 0.0) || (!(sr < 0.0) && (sst >= 0.0));
+  double pk[NEQ];
+#pragma unroll
+  for (int e = 0; e < NEQ; ++e) pk[e] = useL ? pL[e] : pR[e];
+  xflux<NEQ, false>(pk, f, cv);
+  if (!(sl > 0.0) && !(sr < 0.0)) {
+    const double sk = useL ? sl : sr;
+    const double rinv = useL ? rl : rr;
+    const double skmu = sk - pk[1];
+    const double d1 = sk - sst;
+    const double inv = 1.0 / (d1 * skmu);
+    const double rhost = pk[0] * (skmu * skmu) * inv;          // rho (sk-u)/(sk-sst)
+    const double q = pk[4] * rinv * (d1 * inv);                 // p / (rho (sk-u))
+    const double E = 0.5 * pk[0] * (pk[1] * pk[1] + pk[2] * pk[2] + pk[3] * pk[3]) + cv * pk[4];
+    double ust[NEQ], uk[NEQ];
+    prim2flow<NEQ, false>(pk, uk, cv);
+    ust[0] = rhost;
+    ust[1] = rhost * sst;
+    ust[2] = rhost * pk[2];
+    ust[3] = rhost * pk[3];
+    ust[4] = rhost * (E * rinv + (sst - pk[1]) * (sst + q));
+#pragma unroll
+    for (int e = 5; e < NEQ; ++e) ust[e] = rhost * pk[e] * rinv;
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) f[e] = f[e] + sk * (ust[e] - uk[e]);
+  }
+}
 
 // HLL (hll.f90:175-260): Davis wave speeds, branches sl>=0 / sr<=0.
 template <int NEQ, bool MHD>

@@ -28,9 +28,19 @@ struct StageParams {
   PhysParams ph;
 };
 
-template <int NEQ>
-constexpr size_t stage_smem_bytes() {
-  return sizeof(double) * ((size_t)RING * NEQ * HPLANE + 2 * (size_t)NEQ * 17 * NC) + sizeof(DevBlock);
+// Ring channels per cell: the primitives, plus -- for the first-order hydro
+// stage, whose interface states are the cell values -- the sound speed and
+// 1/rho, computed once when the plane is loaded instead of at each of the
+// six interfaces that use the cell.
+template <int NEQ, bool MHD, int ORDER>
+__host__ __device__ constexpr int ring_channels() {
+  return NEQ + ((!MHD && ORDER == 1) ? 2 : 0);
+}
+
+template <int NEQ, bool MHD, int ORDER>
+__host__ __device__ constexpr size_t stage_smem_bytes() {
+  return sizeof(double) * ((size_t)RING * ring_channels<NEQ, MHD, ORDER>() * HPLANE + 2 * (size_t)NEQ * 17 * NC) +
+         sizeof(DevBlock);
 }
 
 __device__ __forceinline__ int hidx(int i, int j) { return (i + 1) + HW * (j + 1); }
@@ -50,8 +60,8 @@ __device__ __forceinline__ void flush_counts(DevCtl* ctl, unsigned pf, unsigned 
 }
 
 // One interface flux in direction DIR from ring cells c0..c3 (pointers to
-// equation 0 of cells l-1, l, r, r+1; stride HPLANE between equations).
-template <int NEQ, bool MHD, int SOLVER, int ORDER, int DIR>
+// equation 0 of cells l-1, l, r, r+1; stride HPLANE between channels).
+template <int NEQ, bool MHD, int SOLVER, int ORDER, int LIM, int DIR>
 __device__ __forceinline__ void iface_flux(const double* c0, const double* c1, const double* c2, const double* c3,
                                            const PhysParams& ph, double* f) {
   double pl[NEQ], pr[NEQ], fx[NEQ];
@@ -67,24 +77,42 @@ __device__ __forceinline__ void iface_flux(const double* c0, const double* c1, c
       const int q = perm<DIR, MHD>(e);
       const double pll = c0[q * HPLANE], prr = c3[q * HPLANE];
       const double dl = pl[e] - pll, dm = pr[e] - pl[e], dr = prr - pr[e];
-      const double al = average(dl, dm, ph.limiter);
-      const double ar = average(dm, dr, ph.limiter);
+      const double al = average_t<LIM>(dl, dm, ph.limiter);
+      const double ar = average_t<LIM>(dm, dr, ph.limiter);
       pl[e] = pl[e] + 0.5 * al;
       pr[e] = pr[e] - 0.5 * ar;
     }
   }
+  if constexpr (!MHD && (SOLVER == WX_SOLVER_HLL || SOLVER == WX_SOLVER_HLLC)) {
+    double cl, cr, rl, rr;
+    if constexpr (ORDER == 1) {  // cell values: sound speed and 1/rho from the ring
+      cl = c1[NEQ * HPLANE];
+      cr = c2[NEQ * HPLANE];
+      rl = c1[(NEQ + 1) * HPLANE];
+      rr = c2[(NEQ + 1) * HPLANE];
+    } else {
+      rl = 1.0 / pl[0];
+      rr = 1.0 / pr[0];
+      cl = sqrt(ph.gamma * pl[4] * rl);
+      cr = sqrt(ph.gamma * pr[4] * rr);
+    }
+    if constexpr (SOLVER == WX_SOLVER_HLLC) riemann_hllc_c<NEQ>(pl, pr, cl, cr, rl, rr, fx, ph.cv);
+    else riemann_hll_c<NEQ>(pl, pr, cl, cr, fx, ph.cv);
+  } else {
 #pragma unroll
-  for (int e = 0; e < NEQ; ++e) fx[e] = 0.0;
-  riemann<NEQ, MHD, SOLVER>(pl, pr, fx, ph.gamma, ph.cv);
+    for (int e = 0; e < NEQ; ++e) fx[e] = 0.0;
+    riemann<NEQ, MHD, SOLVER>(pl, pr, fx, ph.gamma, ph.cv);
+  }
 #pragma unroll
   for (int e = 0; e < NEQ; ++e) f[perm<DIR, MHD>(e)] = fx[e];
 }
 
-template <int NEQ, bool MHD, int SOLVER, int ORDER>
-__global__ void __launch_bounds__(STAGE_THREADS) stage_kernel(StageParams P) {
+template <int NEQ, bool MHD, int SOLVER, int ORDER, int LIM>
+__global__ void __launch_bounds__(STAGE_THREADS, (!MHD && NEQ == 5) ? 2 : 1) stage_kernel(StageParams P) {
+  constexpr int CH = ring_channels<NEQ, MHD, ORDER>();
   extern __shared__ __align__(16) double smem[];
-  double* ring = smem;                                   // [RING][NEQ][HPLANE]
-  double* fxs = ring + RING * NEQ * HPLANE;              // [NEQ][16 rows][17]
+  double* ring = smem;                                   // [RING][CH][HPLANE]
+  double* fxs = ring + RING * CH * HPLANE;               // [NEQ][16 rows][17]
   double* fys = fxs + NEQ * 17 * NC;                     // [NEQ][17][16 cols]
   DevBlock& B = *reinterpret_cast<DevBlock*>(fys + NEQ * 17 * NC);
   const int t = threadIdx.x;
@@ -109,7 +137,7 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel(StageParams P) {
       // ---- load plane kk into the ring (conserved -> primitive) ----------
       __syncthreads();
       {
-        double* pl = ring + ring_slot(kk) * NEQ * HPLANE;
+        double* pl = ring + ring_slot(kk) * CH * HPLANE;
         const bool inner = (kk >= 1 && kk <= NC);
         const bool frame = (kk >= z0 && kk <= z1);  // plane gets x/y fluxes
         const int nframe = frame ? (ORDER == 2 ? 128 : 64) : 0;
@@ -126,10 +154,14 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel(StageParams P) {
             else if (side == 2) { i = r; j = d - 1; }
             else { i = r; j = NC + 2 - d; }
           }
-          double u[NEQ], p[NEQ];
+          double u[NEQ], p[NEQ], rinv;
           if (inner) get_cell<NEQ>(P.src, B, slot, i, j, kk, u);
           else gather_ghost<NEQ>(P.src, B, slot, i, j, kk, u);
-          const int st = flow2prim<NEQ, MHD>(u, p, ph.cv);
+          const int st = flow2prim<NEQ, MHD>(u, p, ph.cv, &rinv);
+          if constexpr (CH > NEQ) {
+            pl[NEQ * HPLANE + hidx(i, j)] = sqrt(ph.gamma * p[4] * rinv);
+            pl[(NEQ + 1) * HPLANE + hidx(i, j)] = rinv;
+          }
           if (c < PLANE && inner && frame) {
             pf += (st == 1);
             df += (st == 2);
@@ -144,19 +176,19 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel(StageParams P) {
       // ---- z-interface m+1/2 of column t ---------------------------------
       if (m >= z0 - 1 && t < PLANE) {
         const int h = hidx(ci, cj);
-        const double* c0 = ring + ring_slot(m - 1) * NEQ * HPLANE + h;
-        const double* c1 = ring + ring_slot(m) * NEQ * HPLANE + h;
-        const double* c2 = ring + ring_slot(m + 1) * NEQ * HPLANE + h;
-        const double* c3 = ring + ring_slot(m + 2) * NEQ * HPLANE + h;
-        iface_flux<NEQ, MHD, SOLVER, ORDER, 2>(c0, c1, c2, c3, ph, znew);
+        const double* c0 = ring + ring_slot(m - 1) * CH * HPLANE + h;
+        const double* c1 = ring + ring_slot(m) * CH * HPLANE + h;
+        const double* c2 = ring + ring_slot(m + 1) * CH * HPLANE + h;
+        const double* c3 = ring + ring_slot(m + 2) * CH * HPLANE + h;
+        iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 2>(c0, c1, c2, c3, ph, znew);
       }
       const bool upd = (m >= z0 && m <= z1);
       if (upd && t < 17 * NC) {
-        const double* pp = ring + ring_slot(m) * NEQ * HPLANE;
+        const double* pp = ring + ring_slot(m) * CH * HPLANE;
         {  // x-interface between ii and ii+1 in row jx
           const int ii = t % 17, jx = t / 17 + 1;
           double f[NEQ];
-          iface_flux<NEQ, MHD, SOLVER, ORDER, 0>(pp + hidx(ii - 1, jx), pp + hidx(ii, jx), pp + hidx(ii + 1, jx),
+          iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 0>(pp + hidx(ii - 1, jx), pp + hidx(ii, jx), pp + hidx(ii + 1, jx),
                                                  pp + hidx(ii + 2, jx), ph, f);
 #pragma unroll
           for (int e = 0; e < NEQ; ++e) fxs[(e * NC + (jx - 1)) * 17 + ii] = f[e];
@@ -164,7 +196,7 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel(StageParams P) {
         {  // y-interface between jj and jj+1 in column iy
           const int iy = (t & 15) + 1, jj = t >> 4;
           double f[NEQ];
-          iface_flux<NEQ, MHD, SOLVER, ORDER, 1>(pp + hidx(iy, jj - 1), pp + hidx(iy, jj), pp + hidx(iy, jj + 1),
+          iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 1>(pp + hidx(iy, jj - 1), pp + hidx(iy, jj), pp + hidx(iy, jj + 1),
                                                  pp + hidx(iy, jj + 2), ph, f);
 #pragma unroll
           for (int e = 0; e < NEQ; ++e) fys[(e * 17 + jj) * NC + (iy - 1)] = f[e];
@@ -177,9 +209,9 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel(StageParams P) {
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) s[e] = 0.0;
         if (MHD && ph.eight_wave) {  // Powell source (sources.f90:38-95) on the stage primitives
-          const double* pm = ring + ring_slot(m) * NEQ * HPLANE;
-          const double* pd = ring + ring_slot(m - 1) * NEQ * HPLANE;
-          const double* pu = ring + ring_slot(m + 1) * NEQ * HPLANE;
+          const double* pm = ring + ring_slot(m) * CH * HPLANE;
+          const double* pd = ring + ring_slot(m - 1) * CH * HPLANE;
+          const double* pu = ring + ring_slot(m + 1) * CH * HPLANE;
           const int h = hidx(ci, cj);
           const double divB = (pm[5 * HPLANE + h + 1] - pm[5 * HPLANE + h - 1]) / (2. * B.dx) +
                               (pm[6 * HPLANE + h + HW] - pm[6 * HPLANE + h - HW]) / (2. * B.dy) +

@@ -82,6 +82,14 @@ class Walicxe3D:
     def set_zsplit(self, z: int):
         self._chk(self.lib.wx3d_set_zsplit(self.ctx, int(z)), "wx3d_set_zsplit")
 
+    def autotune(self, reps: int = 3):
+        """Measured choice of the stage launch shape (z-slab split) for the
+        current mesh; returns (chosen split, {split: ms per predictor+corrector pass})."""
+        ms = (ctypes.c_double * 4)()
+        best = ctypes.c_int32()
+        self._chk(self.lib.wx3d_autotune(self.ctx, int(reps), ms, ctypes.byref(best)), "wx3d_autotune")
+        return best.value, dict(zip((1, 2, 4, 8), list(ms)))
+
     def neighbours(self):
         n = self.nslots
         ft = np.zeros(n * 6, np.int32)
