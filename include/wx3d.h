@@ -267,6 +267,35 @@ int wx3d_reset_status(wx_ctx* ctx);
 int wx3d_hydro_step_noalloc(const wx_config* cfg, int32_t nslots, const int32_t* local_blocks,
                             const double* u_in, double* u_out, wx_state* state, void* cuda_stream);
 
+/*
+ * Learned surrogate of the hydrogen-rate + cooling_h update (one step of
+ * updateNeutralFraction, hrate.f90:82-142, then apply_cooling_h_neq,
+ * cooling_h.f90:154-252): a 4-64-64-2 SiLU MLP with BF16 weights and FP32
+ * accumulation, trained and run by tcgen05 tensor-core kernels.  Inputs are
+ * (log10 n_H, log10 T, x_HII, log10 dt/yr) normalised to [-1,1] over the
+ * box n_H in [1e-3,1e4] cm^-3, T in [1e2,1e8] K, dt in [1e-2,1e3] yr;
+ * outputs are (delta x_HII, delta log10 T / 0.5).  Device pointers are
+ * caller-owned; calls are synchronous.
+ */
+typedef struct wx_mlp wx_mlp;
+int wx3d_mlp_create(uint64_t seed, wx_mlp** out);
+int wx3d_mlp_destroy(wx_mlp* mlp);
+int wx3d_mlp_nparams(void);
+/* parameters, FP32: W1[4][64], b1[64], W2[64][64], b2[64], W3[64][2], b3[2] */
+int wx3d_mlp_get_params(wx_mlp* mlp, float* host_params);
+int wx3d_mlp_set_params(wx_mlp* mlp, const float* host_params);
+/* n samples drawn log-uniformly in the box (x_HII uniform), targets from the
+ * plain FP64 integrator with the rates and scalings of *cfg.  d_in [n][4],
+ * d_target [n][2], d_raw [n][4] = (n_H, T, x_HII, dt in s) or NULL. */
+int wx3d_mlp_samples(const wx_config* cfg, int64_t n, uint64_t seed, float* d_in, float* d_target, double* d_raw,
+                     void* cuda_stream);
+int wx3d_mlp_forward(wx_mlp* mlp, int64_t n, const float* d_in, float* d_out, void* cuda_stream);
+/* loss = mean over samples of the summed squared error; gradient in host_grad */
+int wx3d_mlp_gradient(wx_mlp* mlp, int64_t n, const float* d_in, const float* d_target, float* loss,
+                      float* host_grad);
+int wx3d_mlp_train(wx_mlp* mlp, int64_t n, const float* d_in, const float* d_target, int32_t epochs, int32_t batch,
+                   float lr, float* loss_per_epoch);
+
 /* Human-readable text of a status code and of the context's last error. */
 const char* wx3d_error_string(int32_t code);
 int wx3d_last_error(wx_ctx* ctx, char* buf, int32_t len);

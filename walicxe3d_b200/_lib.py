@@ -19,6 +19,7 @@ _lib = None
 
 c_int32_p = ctypes.POINTER(ctypes.c_int32)
 c_double_p = ctypes.POINTER(ctypes.c_double)
+c_float_p = ctypes.POINTER(ctypes.c_float)
 c_void_p = ctypes.c_void_p
 
 _SIGNATURES = {
@@ -55,6 +56,17 @@ _SIGNATURES = {
     "wx3d_reset_status": (ctypes.c_int, [c_void_p]),
     "wx3d_hydro_step_noalloc": (ctypes.c_int, [ctypes.POINTER(WxConfig), ctypes.c_int32, c_int32_p, c_void_p,
                                                 c_void_p, ctypes.POINTER(WxState), c_void_p]),
+    "wx3d_mlp_create": (ctypes.c_int, [ctypes.c_uint64, ctypes.POINTER(c_void_p)]),
+    "wx3d_mlp_destroy": (ctypes.c_int, [c_void_p]),
+    "wx3d_mlp_nparams": (ctypes.c_int, []),
+    "wx3d_mlp_get_params": (ctypes.c_int, [c_void_p, c_float_p]),
+    "wx3d_mlp_set_params": (ctypes.c_int, [c_void_p, c_float_p]),
+    "wx3d_mlp_samples": (ctypes.c_int, [ctypes.POINTER(WxConfig), ctypes.c_int64, ctypes.c_uint64, c_void_p, c_void_p,
+                                        c_void_p, c_void_p]),
+    "wx3d_mlp_forward": (ctypes.c_int, [c_void_p, ctypes.c_int64, c_void_p, c_void_p, c_void_p]),
+    "wx3d_mlp_gradient": (ctypes.c_int, [c_void_p, ctypes.c_int64, c_void_p, c_void_p, c_float_p, c_float_p]),
+    "wx3d_mlp_train": (ctypes.c_int, [c_void_p, ctypes.c_int64, c_void_p, c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                      ctypes.c_float, c_float_p]),
     "wx3d_error_string": (ctypes.c_char_p, [ctypes.c_int32]),
     "wx3d_last_error": (ctypes.c_int, [c_void_p, ctypes.c_char_p, ctypes.c_int32]),
 }

@@ -1,0 +1,115 @@
+// wx3d_rates.cuh -- device restatement of calcTemp (hydro_core.f90:231-270),
+// the hydrogen rate solution (hrate.f90), the Biro et al. 1999 loss rate
+// (cooling_h.f90) and the cooling-table lookup (cooling.f90).  Inline
+// functions only, so several translation units can include it.
+#pragma once
+
+#include "wx3d_device.cuh"
+
+namespace wx {
+
+constexpr double AMU = 1.660538782e-24;  // source/constants.f90:37
+constexpr double KB = 1.380650400e-16;   // source/constants.f90:38
+
+// calcTemp (hydro_core.f90:231-270)
+template <int FP>
+__device__ __forceinline__ double calc_temp(const double* p, const PhysParams& ph) {
+  double temp = 0.0;
+  switch (ph.eos) {
+    case WX_EOS_ADIABATIC:
+    case WX_EOS_SINGLE_SPECIE: temp = p[4] / p[0] * (ph.mu0 * AMU * ph.p_sc / ph.d_sc / KB); break;
+    case WX_EOS_TWOTEMP:
+      temp = p[4] / p[0] * (ph.mu0 * AMU * ph.p_sc / ph.d_sc / KB);
+      if (temp > ph.ion_thres) temp = p[4] / p[0] * (ph.mui * AMU * ph.p_sc / ph.d_sc / KB);
+      break;
+    case WX_EOS_H_RATE:
+      if (ph.npassive >= 1) temp = p[4] / (2.0 * p[0] / ph.mu0 - p[FP]) * ph.p_sc / KB;
+      break;
+  }
+  return temp;
+}
+
+// solve_h_rate for one cell (hrate.f90:96-137); returns the new neutral
+// fraction y1 for the cell's temperature T and H density dh.
+__device__ __forceinline__ double h_rate_y1(double T, double dh, double y0, double dts) {
+  const double xi = 1.e-4;
+  const double col = 5.83e-11 * sqrt(T) * exp(-157828. / T);   // colf, hrate.f90:73
+  const double rec = 2.55e-13 * pow(1.e4 / T, 0.79);          // alpha, hrate.f90:58
+  const double a = rec + col;
+  const double b = -((2.0 + xi) * rec + (1.0 + xi) * col + 0.0);
+  const double c = (1.0 + xi) * rec;
+  const double d = sqrt(b * b - 4.0 * a * c);
+  const double g0 = (2.0 * a * y0 + b + d) / (2.0 * a * y0 + b - d);
+  const double e = exp(-d * dh * dts);
+  double y1 = (-b - d * (1.0 + g0 * e) / (1.0 - g0 * e)) / (2.0 * a);
+  y1 = dmin(y1, 1.0 - xi);
+  y1 = dmax(y1, 0.0);
+  return y1;
+}
+
+// betah and aloss (cooling_h.f90:42-145), Biro et al. 1999 loss rate.
+__device__ __forceinline__ double betah(double T) {
+  const double a = 157890. / T;
+  return 1.133e-24 / sqrt(a) * (-0.0713 + 0.5 * log(a) + 0.640 * pow(a, -0.33333));
+}
+
+__device__ __forceinline__ double aloss_h(double x1, double den, double dH0, double Te0) {
+  const double XION = 2.179e-11, XO = 1.e-3;
+  const double C0 = 0.5732, C1 = 1.8288e-5, C2 = -1.15822e-10, C3 = 9.4288e-16;
+  const double D0 = 0.5856, D1 = 1.55083e-5, D2 = -9.669e-12, D3 = 5.716e-19;
+  const double ENK = 118409., EN = 1.634E-11;
+  const double Te = dmax(Te0, 10.);
+  const double dHp = (1. - x1) * den;
+  const double de = dHp + 1.E-4 * den;
+  const double dOI = XO * dH0;
+  const double dOII = XO * dHp;
+  if (Te <= 1e4) return 1e-30;
+  double omega;
+  const double oL = C0 + Te * (C1 + Te * (C2 + Te * C3));
+  const double oH = D0 + Te * (D1 + Te * (D2 + Te * D3));
+  if (Te <= 55000.) omega = oL;
+  else if (Te >= 72000.) omega = oH;
+  else {
+    const double frac = (Te - 55000.) / 17000.;
+    omega = (1. - frac) * oL + frac * oH;
+  }
+  const double sTe = sqrt(Te);
+  const double qla = 8.6287E-6 / (2. * sTe) * omega * exp(-ENK / Te);
+  const double ecoll = dmax(de * dH0 * qla * EN, 0.);
+  const double cion = 5.834E-11 * sTe * exp(-1.579E5 / Te);
+  const double eion = de * dH0 * cion * XION;
+  const double erec = dmax(de * dHp * betah(Te), 0.);
+  const double Tm = 1. / Te;
+  const double Tm2 = Tm * Tm;
+  const double eOI = dmax(de * dOI * pow(10., 1381465 * Tm2 - 12328.69 * Tm - 19.82621), 0.);
+  const double eOII = dmax(de * dOII * pow(10., -2061075. * Tm2 - 14596.24 * Tm - 19.01402), 0.);
+  const double betaf = 1.3 * 1.42E-27 * pow(Te, 0.5);
+  const double HIIcool = de * dHp * betaf;
+  const double equil = (1.0455E-18 / pow(Te, 0.63)) * (1. - exp(-pow(Te * 1.E-5, 1.63))) * de * den + HIIcool;
+  double fr;
+  if (Te <= 44770.) fr = 0.;
+  else if (Te >= 54770.) fr = 1.;
+  else {
+    const double ex2 = exp(-2. * (Te - 49770.) / 500.);
+    fr = 0.5 * (1. + (1. - ex2) / (1. + ex2));
+  }
+  return ecoll + eion + (erec + 7.033 * (eOI + eOII)) * (1. - fr) + equil * fr;
+}
+
+// find_coef (cooling.f90:378-419).  The reference scans for the first row
+// whose logT exceeds the argument; on the (increasing) table this is the
+// upper bound found here by bisection.
+__device__ __forceinline__ double find_coef(const double* __restrict__ lt, const double* __restrict__ lc, int n,
+                                            double logT) {
+  if (logT < lt[0]) return 0.0;
+  if (logT >= lt[n - 1]) return pow(10., lc[n - 1] + 0.5 * (logT - lt[n - 1]));
+  int lo = 0, hi = n - 1;  // lt[lo] <= logT < lt[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (lt[mid] > logT) hi = mid; else lo = mid;
+  }
+  const double T0 = lt[hi - 1], C0 = lc[hi - 1], T1 = lt[hi], C1 = lc[hi];
+  return pow(10., (C1 - C0) / (T1 - T0) * (logT - T0) + C0);
+}
+
+}  // namespace wx
