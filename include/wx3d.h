@@ -137,9 +137,12 @@ typedef struct wx_status {
   int64_t nan_cells;       /* non-finite state after a step                     */
   double max_cool_loss;    /* max fractional thermal loss before limiting       */
   int64_t kernels_launched;/* running count of kernels this context launched    */
+  int64_t surrogate_cells; /* cells whose hrate + cooling_h step came from the MLP */
+  int64_t fallback_cells;  /* cells of surrogate steps that used the plain integrator */
 } wx_status;
 
 typedef struct wx_ctx wx_ctx;
+typedef struct wx_mlp wx_mlp;
 
 /* Fills *cfg with the defaults of source/parameters.f90 (HD, HLLC, van Leer,
  * free-flow, CFL 0.4, eta 5e-3) in code units (all scalings 1). */
@@ -207,6 +210,13 @@ int wx3d_hydro_solver(wx_ctx* ctx);
 int wx3d_update_neutral_fraction(wx_ctx* ctx);
 int wx3d_cooling(wx_ctx* ctx, double* maxloss);
 
+/* updatePrims + updateNeutralFraction + cooling (source/main.f90:94-100)
+ * fused in one pass over U with the current dt, the source part of
+ * wx3d_step; uses the surrogate when one is attached.  Also folds the CFL
+ * minimum for the next step.  maxloss as for wx3d_cooling.  No reference
+ * counterpart as one call. */
+int wx3d_sources(wx_ctx* ctx, double* maxloss);
+
 /* One main-loop iteration without AMR and output (source/main.f90:81-100):
  * it += 1, hydroSolver, updatePrims, updateNeutralFraction (EOS_H_RATE),
  * cooling.  *out (may be NULL) receives the state after the step. */
@@ -270,14 +280,14 @@ int wx3d_hydro_step_noalloc(const wx_config* cfg, int32_t nslots, const int32_t*
 /*
  * Learned surrogate of the hydrogen-rate + cooling_h update (one step of
  * updateNeutralFraction, hrate.f90:82-142, then apply_cooling_h_neq,
- * cooling_h.f90:154-252): a 4-64-64-2 SiLU MLP with BF16 weights and FP32
- * accumulation, trained and run by tcgen05 tensor-core kernels.  Inputs are
- * (log10 n_H, log10 T, x_HII, log10 dt/yr) normalised to [-1,1] over the
- * box n_H in [1e-3,1e4] cm^-3, T in [1e2,1e8] K, dt in [1e-2,1e3] yr;
- * outputs are (delta x_HII, delta log10 T / 0.5).  Device pointers are
- * caller-owned; calls are synchronous.
+ * cooling_h.f90:154-252): a 4-64-64-2 SiLU MLP with BF16 operands and FP32
+ * accumulation, trained and run by tcgen05 tensor-core kernels (forward
+ * hidden layers as BF16 head + tail products, FP32 output layer).  Inputs
+ * are (log10 n_H dt/yr, log10 T, x_HII, log10 dt/yr) normalised to [-1,1]
+ * over the box n_H in [1e-3,1e4] cm^-3, T in [1e2,1e8] K, dt in
+ * [1e-2,1e3] yr; outputs are (delta x_HII / 0.125, log10(P1/P0) / log10 2).
+ * Device pointers are caller-owned; calls are synchronous.
  */
-typedef struct wx_mlp wx_mlp;
 int wx3d_mlp_create(uint64_t seed, wx_mlp** out);
 int wx3d_mlp_destroy(wx_mlp* mlp);
 int wx3d_mlp_nparams(void);
@@ -295,6 +305,14 @@ int wx3d_mlp_gradient(wx_mlp* mlp, int64_t n, const float* d_in, const float* d_
                       float* host_grad);
 int wx3d_mlp_train(wx_mlp* mlp, int64_t n, const float* d_in, const float* d_target, int32_t epochs, int32_t batch,
                    float lr, float* loss_per_epoch);
+
+/* Attaches (enable = 1) the surrogate to a context whose config is
+ * EOS_H_RATE + COOL_H: the source step of wx3d_step / wx3d_run then uses the
+ * MLP for the cells in the trust box whose bin of `trust` is non-zero, and
+ * the plain integrator elsewhere.  trust[24][24][4] (nbytes = 2304) bins
+ * log10(n_H dt/yr) in [-5,7) by 0.5, log10 T in [2,8) by 0.25 and x_HII in
+ * quarters.  enable = 0 detaches it. */
+int wx3d_set_surrogate(wx_ctx* ctx, wx_mlp* mlp, const uint8_t* trust, int32_t nbytes, int32_t enable);
 
 /* Human-readable text of a status code and of the context's last error. */
 const char* wx3d_error_string(int32_t code);

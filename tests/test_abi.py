@@ -32,7 +32,7 @@ def test_struct_sizes_match_header():
     # wx_config: 17 int32 fields (+ 5 for bc[6] beyond one) then 17 doubles
     assert ctypes.sizeof(WxConfig) == 4 * 20 + 8 * 17
     assert ctypes.sizeof(WxState) == 32
-    assert ctypes.sizeof(WxStatus) == 48
+    assert ctypes.sizeof(WxStatus) == 64
 
 
 def test_config_defaults_match_parameters_f90():

@@ -59,7 +59,7 @@ def test_samples_match_cpu_integrator(ncpu):
     import oracle
     from walicxe3d_b200 import problems
     from walicxe3d_b200.config import KB
-    from walicxe3d_b200.surrogate import SCALE_T, samples
+    from walicxe3d_b200.surrogate import SCALE_C, SCALE_X, samples
 
     prob = problems.snr_h(nroot=1, maxlev=1)
     cfg = prob.cfg
@@ -91,8 +91,8 @@ def test_samples_match_cpu_integrator(ncpu):
         o.cooling()
         pr = o.PRIM[0]
         y1 = pr[5].ravel()[k] / dh[k]
-        T1 = pr[4].ravel()[k] * cfg.p_sc / (KB * dh[k] * (2.0 - y1))
-        res_ok.append((abs((1 - y1) - xh[k] - t[k, 0]), abs(np.log10(T1 / T0[k]) / SCALE_T - t[k, 1])))
+        cf = pr[4].ravel()[k] / P.ravel()[k]
+        res_ok.append((abs(((1 - y1) - xh[k]) / SCALE_X - t[k, 0]), abs(np.log10(cf) / SCALE_C - t[k, 1])))
     err = np.array(res_ok)
     assert err[:, 0].max() < 1e-6 and err[:, 1].max() < 1e-6, err
 

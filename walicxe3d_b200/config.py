@@ -100,6 +100,8 @@ class WxStatus(ctypes.Structure):
         ("nan_cells", ctypes.c_int64),
         ("max_cool_loss", ctypes.c_double),
         ("kernels_launched", ctypes.c_int64),
+        ("surrogate_cells", ctypes.c_int64),
+        ("fallback_cells", ctypes.c_int64),
     ]
 
 

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../../include/wx3d.h"
+#include "wx3d_internal.h"
 #include "wx3d_kernels.cuh"
 #include "wx3d_source.cuh"
 
@@ -166,6 +167,10 @@ struct wx_ctx {
   cudaGraphExec_t graph = nullptr;
   bool graph_valid = false;
   long long launches = 0;
+  // learned surrogate of hrate + cooling_h (wx3d_set_surrogate)
+  const wx_mlp* mlp = nullptr;
+  uint8_t* dTrust = nullptr;
+  bool use_surrogate = false;
   // per-kernel timing: event pairs around the launches of one step sequence
   bool timing = false;
   bool timing_mute = false;
@@ -250,8 +255,12 @@ void tick(wx_ctx* c, int kind, bool begin) {
   if (!c->timing || c->timing_mute || c->nev >= 64) return;
   if (begin) c->ev_kind[c->nev / 2] = kind;
   // external record: inside a stream capture this becomes an event-record
-  // node of the graph, so the replay itself stamps the event
-  cudaEventRecordWithFlags(c->ev[c->nev], c->stream, cudaEventRecordExternal);
+  // node of the graph, so the replay itself stamps the event; outside a
+  // capture the flag is not allowed and a plain record is used
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(c->stream, &cs);
+  cudaEventRecordWithFlags(c->ev[c->nev], c->stream,
+                           cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault);
   ++c->nev;
 }
 
@@ -344,6 +353,19 @@ int enqueue_sources(wx_ctx* c, int mode) {
   return WX_OK;
 }
 
+int enqueue_surrogate(wx_ctx* c) {
+  ctl_reset_dtmin_kernel<<<1, 1, 0, c->stream>>>(c->dCtl);
+  WX_LAUNCHED();
+  SurrLaunch L{c->neq, c->dU, c->dBlocks, c->dWork, c->nwork, c->dCtl, c->ph, c->mlp, c->dTrust, 1, c->nsm};
+  tick(c, 3, true);
+  const cudaError_t e = launch_surrogate_source(L, c->stream);
+  if (e != cudaSuccess) return fail(c, WX_ERR_CUDA, "surrogate launch: %s", cudaGetErrorString(e));
+  ++c->launches;
+  tick(c, 3, false);
+  c->dt_valid = true;
+  return WX_OK;
+}
+
 int enqueue_step(wx_ctx* c) {
   int rc;
   if (!c->dt_valid) {
@@ -351,6 +373,7 @@ int enqueue_step(wx_ctx* c) {
     c->dt_valid = true;
   }
   if ((rc = enqueue_solver(c, true, true))) return rc;
+  if (c->use_surrogate) return enqueue_surrogate(c);
   if (sources_on(c)) {
     int mode = 8;
     if (c->cfg.eos_type == WX_EOS_H_RATE) mode |= 1;
@@ -479,6 +502,7 @@ int wx3d_finalize(wx_ctx* c) {
   invalidate_graph(c);
   cudaFree(c->dU); cudaFree(c->dUP); cudaFree(c->dW); cudaFree(c->dPrim); cudaFree(c->dStage);
   cudaFree(c->dBlocks); cudaFree(c->dWork); cudaFree(c->dFlags); cudaFree(c->dCtl); cudaFree(c->dCool);
+  cudaFree(c->dTrust);
   if (c->hCtl) cudaFreeHost(c->hCtl);
   for (int i = 0; i < 64; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -805,6 +829,26 @@ int wx3d_cooling(wx_ctx* c, double* maxloss) {
   return WX_OK;
 }
 
+// updatePrims + updateNeutralFraction + cooling fused in one pass over U (the
+// source part of wx3d_step), with the surrogate when one is attached.
+int wx3d_sources(wx_ctx* c, double* maxloss) {
+  if (!ready(c)) return fail(c, WX_ERR_MESH, "no mesh");
+  int rc;
+  c->nev = 0;
+  WX_CUDA(cudaMemsetAsync(&c->dCtl->maxloss_bits, 0, 8, c->stream));
+  if (c->use_surrogate) {
+    if ((rc = enqueue_surrogate(c))) return rc;
+  } else if (sources_on(c)) {
+    int mode = 8;
+    if (c->cfg.eos_type == WX_EOS_H_RATE) mode |= 1;
+    if (c->cfg.cooling_type != WX_COOL_NONE) mode |= 2;
+    if ((rc = enqueue_sources(c, mode))) return rc;
+  }
+  if ((rc = sync_check(c))) return rc;
+  if (maxloss) std::memcpy(maxloss, &c->hCtl->maxloss_bits, 8);
+  return WX_OK;
+}
+
 int wx3d_step(wx_ctx* c, wx_state* out) {
   if (!ready(c)) return fail(c, WX_ERR_MESH, "no mesh");
   const int dumps0 = c->hCtl->dumps;
@@ -966,6 +1010,28 @@ int wx3d_kernel_times(wx_ctx* c, double* ms4, int32_t* count4) {
   return WX_OK;
 }
 
+// Attaches (enable=1) or detaches the learned surrogate of hrate + cooling_h.
+int wx3d_set_surrogate(wx_ctx* c, wx_mlp* mlp, const uint8_t* trust, int32_t nbytes, int32_t enable) {
+  if (!c) return WX_ERR_INVALID_ARG;
+  if (!enable) {
+    c->use_surrogate = false;
+    invalidate_graph(c);
+    return WX_OK;
+  }
+  if (!mlp || !trust || nbytes != TRUST_BYTES) return fail(c, WX_ERR_INVALID_ARG, "surrogate needs a %d-byte trust table", TRUST_BYTES);
+  const wx_config& f = c->cfg;
+  if (f.eos_type != WX_EOS_H_RATE || f.cooling_type != WX_COOL_H || f.bfield || f.npassive < 1 || f.neqtot > 7)
+    return fail(c, WX_ERR_UNSUPPORTED, "the surrogate replaces EOS_H_RATE + COOL_H in hydro runs with 1-2 passives");
+  if (f.cooling_limit != 0.5)
+    return fail(c, WX_ERR_UNSUPPORTED, "the surrogate was trained with cooling_limit = 0.5");
+  if (!c->dTrust) WX_CUDA(cudaMalloc(&c->dTrust, TRUST_BYTES));
+  WX_CUDA(cudaMemcpy(c->dTrust, trust, TRUST_BYTES, cudaMemcpyHostToDevice));
+  c->mlp = mlp;
+  c->use_surrogate = true;
+  invalidate_graph(c);
+  return WX_OK;
+}
+
 int wx3d_get_status(wx_ctx* c, wx_status* st) {
   if (!c || !st) return WX_ERR_INVALID_ARG;
   WX_CUDA(cudaMemcpyAsync(c->hCtl, c->dCtl, sizeof(DevCtl), cudaMemcpyDeviceToHost, c->stream));
@@ -976,12 +1042,15 @@ int wx3d_get_status(wx_ctx* c, wx_status* st) {
   st->nan_cells = (int64_t)c->hCtl->cnt[3];
   std::memcpy(&st->max_cool_loss, &c->hCtl->maxloss_bits, 8);
   st->kernels_launched = c->launches;
+  st->surrogate_cells = (int64_t)c->hCtl->sur[0];
+  st->fallback_cells = (int64_t)c->hCtl->sur[1];
   return WX_OK;
 }
 
 int wx3d_reset_status(wx_ctx* c) {
   if (!c) return WX_ERR_INVALID_ARG;
   WX_CUDA(cudaMemsetAsync(&c->dCtl->cnt[0], 0, sizeof(c->hCtl->cnt) + 8, c->stream));
+  WX_CUDA(cudaMemsetAsync(&c->dCtl->sur[0], 0, sizeof(c->hCtl->sur), c->stream));
   WX_CUDA(cudaStreamSynchronize(c->stream));
   return WX_OK;
 }

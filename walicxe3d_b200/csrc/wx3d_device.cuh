@@ -47,6 +47,7 @@ struct __align__(16) DevCtl {
   int32_t dumps;                  // outputs that fell inside a batched run
   unsigned long long cnt[4];      // pressure floor, density floor, zero density, non-finite
   unsigned long long maxloss_bits;
+  unsigned long long sur[2];      // cells updated by the surrogate / by the plain integrator
 };
 
 struct PhysParams {

@@ -1,13 +1,22 @@
 // wx3d_mlp.cu -- learned surrogate for the hydrogen-rate + cooling_h update.
 //
 // A 4 -> 64 -> 64 -> 2 MLP with SiLU activations maps
-//   (log10 n_H, log10 T, x_HII, log10 dt/yr)  ->  (delta x_HII, delta log10 T)
+//   (log10 n_H dt/yr, log10 T, x_HII, log10 dt/yr)
+//      ->  (delta x_HII / SCALE_X, log10(cooling factor) / SCALE_C)
 // for one step of updateNeutralFraction (hrate.f90:82-142) followed by
-// apply_cooling_h_neq (cooling_h.f90:154-252).  Weights are BF16, products
-// accumulate in FP32 in tensor memory: every layer, forward and backward,
-// is a tcgen05.mma (kind::f16, M=128) issued by one thread, with operands in
-// shared memory in the canonical no-swizzle core-matrix layout and the
-// accumulator in TMEM, read back with tcgen05.ld.
+// apply_cooling_h_neq (cooling_h.f90:154-252); the cooling factor is the
+// ratio of the pressures after and before the step, so the new state is
+// P1 = cf * P0 and n_HI = n_H (1 - x1), as the plain step writes it.
+//
+// Operands are BF16, products accumulate in FP32 in tensor memory: the two
+// hidden layers, and every product of the backward pass, are tcgen05.mma
+// (kind::f16, M=128) issued by one thread, with operands in shared memory in
+// the canonical no-swizzle core-matrix layout and the accumulator in TMEM,
+// read back with tcgen05.ld.  In the forward pass the inputs, W1, the first
+// hidden layer and W2 are split into a BF16 head and a BF16 tail
+// (a = hi + lo, lo = bf16(a - hi)) and each layer sums the three products
+// hi*hi + lo*hi + hi*lo, which carries about 16 significant bits instead of
+// 8.  The 64 -> 2 output layer is an FP32 dot product on the CUDA cores.
 //
 // Operand layout.  A matrix of R rows and C columns (bf16) is stored as a
 // grid of 8x8 "core matrices" of 128 bytes: element (r, c) lives at byte
@@ -34,6 +43,7 @@
 #include <vector>
 
 #include "../../include/wx3d.h"
+#include "wx3d_internal.h"
 #include "wx3d_rates.cuh"
 
 namespace wx {
@@ -46,13 +56,16 @@ constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + NIN * NH, OFF_W2 = OFF_B1 + NH, OFF_
 constexpr int OFF_W3 = OFF_B2 + NH, OFF_B3 = OFF_W3 + NH * NOUT, NPARAM = OFF_B3 + NOUT;
 
 // Packed bf16 operand images of the weights (core-matrix layout):
-//   W1B  [N=64 ][K=16]  (n,k) = W1[k][n]   (k<4), B of layer 1
-//   W2B  [N=64 ][K=64]  (n,k) = W2[k][n],         B of layer 2
-//   W3B  [N=16 ][K=64]  (n,k) = W3[k][n]   (n<2), B of layer 3
+//   W1B  [N=64 ][K=16]  (n,k) = hi(W1[k][n]) k<4, 0 at k=4, hi(W1[k-5][n])
+//                       for 5<=k<9, lo(W1[k-9][n]) for 9<=k<13: B of layer 1,
+//                       against input rows (hi(x), 1, lo(x), hi(x))
+//   W2B  [N=64 ][K=64]  (n,k) = hi(W2[k][n]),     B of layer 2
+//   W2L  [N=64 ][K=64]  (n,k) = lo(W2[k][n]),     B of layer 2 (tail)
 //   W3R  [N=64 ][K=16]  (n,k) = W3[n][k]   (k<2), B of dH2 = dY W3^T
 //   W2R  [N=64 ][K=64]  (n,k) = W2[n][k],         B of dH1 = dZ2 W2^T
-constexpr int PK_W1B = 0, PK_W2B = PK_W1B + 64 * 16, PK_W3B = PK_W2B + 64 * 64, PK_W3R = PK_W3B + 16 * 64,
+constexpr int PK_W1B = 0, PK_W2B = PK_W1B + 64 * 16, PK_W2L = PK_W2B + 64 * 64, PK_W3R = PK_W2L + 64 * 64,
               PK_W2R = PK_W3R + 64 * 16, PK_N = PK_W2R + 64 * 64;   // bf16 elements
+constexpr int PK_INF = PK_W3R;                                      // forward-only prefix
 
 __host__ __device__ constexpr int cm_off(int r, int c, int C) {  // element offset in a core-matrix grid
   return (((r >> 3) * (C >> 3) + (c >> 3)) << 6) + ((r & 7) << 3) + (c & 7);
@@ -158,9 +171,24 @@ __device__ __forceinline__ void put8(__nv_bfloat16* m, int r, int c, int C, cons
   *reinterpret_cast<uint4*>(m + cm_off(r, c, C)) = *reinterpret_cast<const uint4*>(q);
 }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// Writes 8 consecutive values of row r (c % 8 == 0) as their bf16 head into
+// hi and their bf16 tail into lo (lo may have another column count CL).
+__device__ __forceinline__ void put8_split(__nv_bfloat16* hi, int C, __nv_bfloat16* lo, int CL, int r, int c,
+                                           const float* v) {
+  __align__(16) __nv_bfloat162 qh[4], ql[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    qh[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+    const float2 f = __bfloat1622float2(qh[i]);
+    ql[i] = __floats2bfloat162_rn(v[2 * i] - f.x, v[2 * i + 1] - f.y);
+  }
+  *reinterpret_cast<uint4*>(hi + cm_off(r, c, C)) = *reinterpret_cast<const uint4*>(qh);
+  *reinterpret_cast<uint4*>(lo + cm_off(r, c, CL)) = *reinterpret_cast<const uint4*>(ql);
+}
+
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float dsilu(float z) {
-  const float s = 1.0f / (1.0f + __expf(-z));
+  const float s = __fdividef(1.0f, 1.0f + __expf(-z));
   return s * (1.0f + z * (1.0f - s));
 }
 
@@ -170,46 +198,38 @@ struct Box {
   static constexpr double LN_LO = -3.0, LN_HI = 4.0;    // log10 n_H  [cm^-3]
   static constexpr double LT_LO = 2.0, LT_HI = 8.0;     // log10 T    [K]
   static constexpr double LD_LO = -2.0, LD_HI = 3.0;    // log10 dt   [yr]
-  static constexpr double SCALE_T = 0.5;                // delta log10 T is learned as 2 * value
+  static constexpr double SCALE_X = 0.125;              // output 0 = delta x_HII / SCALE_X
+  static constexpr double SCALE_C = 0.30102999566398120;  // output 1 = log10(cf) / log10(2)
 };
 
-__host__ __device__ inline void normalise(double lgn, double lgT, double x, double lgdt, float* in) {
-  in[0] = (float)((lgn - 0.5 * (Box::LN_LO + Box::LN_HI)) / (0.5 * (Box::LN_HI - Box::LN_LO)));
-  in[1] = (float)((lgT - 0.5 * (Box::LT_LO + Box::LT_HI)) / (0.5 * (Box::LT_HI - Box::LT_LO)));
-  in[2] = (float)(2.0 * x - 1.0);
-  in[3] = (float)((lgdt - 0.5 * (Box::LD_LO + Box::LD_HI)) / (0.5 * (Box::LD_HI - Box::LD_LO)));
+// Network inputs in [-1, 1]: log10(n_H dt/yr) over [-5, 7] (the rates of
+// hrate.f90 and the losses of cooling_h.f90 depend on n_H and dt only
+// through their product), log10 T, x_HII and log10 dt/yr.
+template <class F>
+__host__ __device__ inline void normalise(F lgn, F lgT, F x, F lgdt, float* in) {
+  constexpr double ND_LO = Box::LN_LO + Box::LD_LO, ND_HI = Box::LN_HI + Box::LD_HI;
+  in[0] = (float)((lgn + lgdt - F(0.5 * (ND_LO + ND_HI))) * F(2.0 / (ND_HI - ND_LO)));
+  in[1] = (float)((lgT - F(0.5 * (Box::LT_LO + Box::LT_HI))) * F(2.0 / (Box::LT_HI - Box::LT_LO)));
+  in[2] = (float)(F(2) * x - F(1));
+  in[3] = (float)((lgdt - F(0.5 * (Box::LD_LO + Box::LD_HI))) * F(2.0 / (Box::LD_HI - Box::LD_LO)));
 }
 
-// One plain FP64 step of hrate then cooling_h for a cell with H density dh,
-// neutral fraction y0 and temperature T0 (EOS_H_RATE: P = T k dh (2-y) / p_sc).
-// Returns y1 and T1 (the temperature of the updated state).  This is the
-// arithmetic of source_kernel's hrate and COOL_H branches.
+// One plain FP64 step of hrate then cooling_h for a cell at rest with H
+// density dh, neutral fraction y0 and temperature T0 (EOS_H_RATE:
+// P = T k dh (2-y) / p_sc).  Returns y1 and the cooling factor P1/P0.
 __device__ inline void plain_h_update(double dh, double y0, double T0, double dts, const PhysParams& ph, double* y1o,
-                                      double* T1o) {
-  const double P0 = T0 * KB * dh * (2.0 - y0) / ph.p_sc;
-  double p[6];
+                                      double* cfo) {
+  double u[6], p[6];
   p[0] = dh * ph.mu0;
-  p[4] = P0;
+  p[1] = p[2] = p[3] = 0.0;
+  p[4] = T0 * KB * dh * (2.0 - y0) / ph.p_sc;
   p[5] = dh * y0;
-  // hrate.f90:106-131
-  const double T = calc_temp<5>(p, ph);
-  const double y1 = h_rate_y1(T, dh, p[5] / dh, dts);
-  p[5] = p[0] * y1 / ph.mu0;
-  // cooling_h.f90:180-244 (U(firstpas) still holds the old neutral density)
-  const double dh0 = p[5];
-  const double yold = y0;
-  const double Temp = calc_temp<5>(p, ph);
-  if (Temp > 1.e4) {
-    const double L0 = aloss_h(yold, dh, dh0, Temp);
-    const double ce = (2.0 * L0) / (3.0 * KB * dh * Temp);
-    const double T1 = 10.0 + (Temp - 10.0) * exp(-ce * dts);
-    double cf = T1 / Temp;
-    if (cf < 1.0 - ph.cooling_limit) cf = 1.0 - ph.cooling_limit;
-    if (Temp * cf < 10.0) cf = 10.0 / Temp;
-    p[4] = p[4] * cf;
-  }
-  *y1o = y1;
-  *T1o = calc_temp<5>(p, ph);
+  prim2flow<6, false>(p, u, ph.cv);
+  const double p4 = p[4];
+  double ml = 0.0;
+  h_cool_step<5>(u, p, dts, ph, &ml);
+  *y1o = p[5] / (p[0] / ph.mu0);
+  *cfo = p[4] / p4;
 }
 
 // ---------------------------------------------------------------------------
@@ -233,13 +253,11 @@ __global__ void sample_kernel(PhysParams ph, long long n, unsigned long long see
     const double x = u01(seed, i, 2);
     const double lgd = Box::LD_LO + (Box::LD_HI - Box::LD_LO) * u01(seed, i, 3);
     const double dh = pow(10.0, lgn), T0 = pow(10.0, lgT), dts = pow(10.0, lgd) * 3.155673600e+7;
-    double y1, T1;
-    plain_h_update(dh, 1.0 - x, T0, dts, ph, &y1, &T1);
+    double y1, cf;
+    plain_h_update(dh, 1.0 - x, T0, dts, ph, &y1, &cf);
     normalise(lgn, lgT, x, lgd, in + 4 * i);
-    const double dx = (1.0 - y1) - x;
-    const double dlt = log10(T1 / T0);
-    out[2 * i] = (float)dx;
-    out[2 * i + 1] = (float)(dlt / Box::SCALE_T);
+    out[2 * i] = (float)(((1.0 - y1) - x) / Box::SCALE_X);
+    out[2 * i + 1] = (float)(log10(cf) / Box::SCALE_C);
     if (raw) {
       raw[4 * i] = dh; raw[4 * i + 1] = T0; raw[4 * i + 2] = x; raw[4 * i + 3] = dts;
     }
@@ -247,18 +265,38 @@ __global__ void sample_kernel(PhysParams ph, long long n, unsigned long long see
 }
 
 // ---------------------------------------------------------------------------
-// Shared memory of one MLP tile
+// Shared memory.  FwdSmem is the training kernel's forward image (hidden
+// activations padded to 128 columns for the weight-gradient MMAs); InfSmem
+// is the inference image (64-column hidden layer 1, no layer-2 buffer: the
+// 64 -> 2 output layer runs on the CUDA cores in FP32).
 
 struct __align__(128) FwdSmem {
-  __nv_bfloat16 x[TILE * 16];     // [128][16]  inputs (col 4 = 1 for the dW1 bias row)
-  __nv_bfloat16 h1[TILE * 128];   // [128][128] SiLU(z1), cols 64.. = (1, 0, ...)
+  __nv_bfloat16 x[TILE * 16];     // [128][16]  inputs hi(x), 1 (dW1 bias row), lo(x), hi(x)
+  __nv_bfloat16 h1[TILE * 128];   // [128][128] hi(SiLU(z1)), cols 64.. = (1, 0, ...)
+  __nv_bfloat16 h1lo[TILE * 64];  // [128][64]  lo(SiLU(z1))
   __nv_bfloat16 h2[TILE * 128];   // [128][128] SiLU(z2), cols 64.. = (1, 0, ...)
   __nv_bfloat16 w[PK_N];          // packed weights
-  float b1[NH], b2[NH], b3[16];
+  float b1[NH], b2[NH], w3[NH * NOUT], b3[16];
   uint64_t bar;
   uint32_t tmem;
   int err;
 };
+
+struct __align__(128) InfSmem {
+  __nv_bfloat16 x[TILE * 16];     // [128][16]  inputs hi(x), 1, lo(x), hi(x)
+  __nv_bfloat16 h1[TILE * 64];    // [128][64]  hi(SiLU(z1))
+  __nv_bfloat16 h1lo[TILE * 64];  // [128][64]  lo(SiLU(z1))
+  __nv_bfloat16 w[PK_INF];        // W1B, W2B, W2L
+  float b1[NH], b2[NH], w3[NH * NOUT], b3[16];
+  uint64_t bar;
+  uint32_t tmem;
+  int err;
+};
+// Inference CTAs allocate 128 TMEM columns; the dynamic shared memory of an
+// inference launch is padded so that at most four CTAs share an SM and
+// their allocations (4 x 128 of 512 columns) never wait on each other.
+constexpr size_t INF_SMEM = 56 * 1024;
+static_assert(sizeof(InfSmem) <= INF_SMEM, "inference shared memory");
 
 struct __align__(128) BwdSmem {
   __nv_bfloat16 dy[TILE * 16];    // [128][16]  output gradient (cols 0,1)
@@ -266,15 +304,17 @@ struct __align__(128) BwdSmem {
   __nv_bfloat16 dz1[TILE * 128];  // [128][128] cols 64.. zero (M padding of dW1^T)
 };
 
-// Loads the packed weights and biases into shared memory.
-__device__ void load_weights(FwdSmem& s, const __nv_bfloat16* __restrict__ pk, const float* __restrict__ prm) {
+// Loads the first nw packed weights and the FP32 biases and output layer.
+template <class S>
+__device__ void load_weights(S& s, const __nv_bfloat16* __restrict__ pk, const float* __restrict__ prm, int nw) {
   const uint4* src = reinterpret_cast<const uint4*>(pk);
   uint4* dst = reinterpret_cast<uint4*>(s.w);
-  for (int i = threadIdx.x; i < PK_N / 8; i += blockDim.x) dst[i] = src[i];
+  for (int i = threadIdx.x; i < nw / 8; i += blockDim.x) dst[i] = src[i];
   for (int i = threadIdx.x; i < NH; i += blockDim.x) {
     s.b1[i] = prm[OFF_B1 + i];
     s.b2[i] = prm[OFF_B2 + i];
   }
+  for (int i = threadIdx.x; i < NH * NOUT; i += blockDim.x) s.w3[i] = prm[OFF_W3 + i];
   if (threadIdx.x < 16) s.b3[threadIdx.x] = threadIdx.x < NOUT ? prm[OFF_B3 + threadIdx.x] : 0.f;
 }
 
@@ -290,14 +330,19 @@ __device__ __forceinline__ void pad_row(__nv_bfloat16* m, int r) {
   for (int c = 72; c < 128; c += 8) put8(m, r, c, 128, v);
 }
 
-// Forward pass of one tile whose inputs are already in s.x.  TMEM columns:
-// [0,64) z1, [64,128) z2, [128,144) y.  On return (all threads) y[0..1] holds
-// this thread's outputs and z1/z2 stay in TMEM.  Returns false on timeout.
-__device__ bool forward_tile(FwdSmem& s, uint32_t& phase, float* y) {
+// Forward pass of one tile whose inputs are already in s.x.  Layers 1 and 2
+// are tcgen05 MMAs into TMEM columns [0,64) (z1) and [64,128) (z2), layer 2
+// as the 12 K-steps hi(h1) hi(W2) + lo(h1) hi(W2) + hi(h1) lo(W2); the
+// output layer is an FP32 dot product of this thread's SiLU(z2) row with
+// W3.  HC is the column count of s.h1; KEEP stores SiLU(z2) (bf16) in h2s
+// for the weight gradients.  On return y[0..1] holds this thread's outputs
+// and z1/z2 stay in TMEM.  Returns false (uniformly) on timeout.
+template <int HC, bool KEEP, class S>
+__device__ bool forward_tile(S& s, __nv_bfloat16* h2s, uint32_t& phase, float* y) {
   const int t = threadIdx.x;
   const uint32_t tb = s.tmem;
-  const uint32_t xa = smem_u32(s.x), h1a = smem_u32(s.h1), h2a = smem_u32(s.h2), wa = smem_u32(s.w);
-  // layer 1: [128 x 16] x W1B -> z1
+  const uint32_t xa = smem_u32(s.x), h1a = smem_u32(s.h1), h1l = smem_u32(s.h1lo), wa = smem_u32(s.w);
+  // layer 1: [128 x 16] x W1B -> z1 (the three products are K columns)
   fence_async_smem();
   fence_before();
   __syncthreads();
@@ -319,10 +364,10 @@ __device__ bool forward_tile(FwdSmem& s, uint32_t& phase, float* y) {
       float h[8];
 #pragma unroll
       for (int i = 0; i < 8; ++i) h[i] = silu(z[8 * q + i] + s.b1[8 * q + i]);
-      put8(s.h1, t, 8 * q, 128, h);
+      put8_split(s.h1, HC, s.h1lo, 64, t, 8 * q, h);
     }
   }
-  // layer 2: [128 x 64] x W2B -> z2
+  // layer 2: [128 x 64] x (W2B + W2L) -> z2
   fence_async_smem();
   fence_before();
   __syncthreads();
@@ -330,8 +375,16 @@ __device__ bool forward_tile(FwdSmem& s, uint32_t& phase, float* y) {
     fence_after();
 #pragma unroll
     for (int j = 0; j < 4; ++j)
-      mma_bf16(tb + 64, sdesc(h1a + 256 * j, 128, 16 * 128), sdesc(wa + 2 * PK_W2B + 256 * j, 128, 8 * 128),
+      mma_bf16(tb + 64, sdesc(h1a + 256 * j, 128, (HC / 8) * 128), sdesc(wa + 2 * PK_W2B + 256 * j, 128, 8 * 128),
                idesc(128, 64, 0, 0), j > 0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      mma_bf16(tb + 64, sdesc(h1l + 256 * j, 128, 8 * 128), sdesc(wa + 2 * PK_W2B + 256 * j, 128, 8 * 128),
+               idesc(128, 64, 0, 0), 1);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      mma_bf16(tb + 64, sdesc(h1a + 256 * j, 128, (HC / 8) * 128), sdesc(wa + 2 * PK_W2L + 256 * j, 128, 8 * 128),
+               idesc(128, 64, 0, 0), 1);
     mma_commit(&s.bar);
   }
   if (!__syncthreads_and(mbar_wait(&s.bar, phase))) return false;
@@ -342,59 +395,56 @@ __device__ bool forward_tile(FwdSmem& s, uint32_t& phase, float* y) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) tmem_ld16(tmem_addr(tb, 64 + 16 * q), z + 16 * q);
     tmem_wait_ld();
+    float y0 = s.b3[0], y1 = s.b3[1];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       float h[8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) h[i] = silu(z[8 * q + i] + s.b2[8 * q + i]);
-      put8(s.h2, t, 8 * q, 128, h);
+      for (int i = 0; i < 8; ++i) {
+        const int j = 8 * q + i;
+        h[i] = silu(z[j] + s.b2[j]);
+        y0 = fmaf(h[i], s.w3[2 * j], y0);
+        y1 = fmaf(h[i], s.w3[2 * j + 1], y1);
+      }
+      if (KEEP) put8(h2s, t, 8 * q, 128, h);
     }
-  }
-  // layer 3: [128 x 64] x W3B -> y (N = 16, two used)
-  fence_async_smem();
-  fence_before();
-  __syncthreads();
-  if (t == 0) {
-    fence_after();
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-      mma_bf16(tb + 128, sdesc(h2a + 256 * j, 128, 16 * 128), sdesc(wa + 2 * PK_W3B + 256 * j, 128, 8 * 128),
-               idesc(128, 16, 0, 0), j > 0);
-    mma_commit(&s.bar);
-  }
-  if (!__syncthreads_and(mbar_wait(&s.bar, phase))) return false;
-  phase ^= 1;
-  fence_after();
-  {
-    float v[16];
-    tmem_ld16(tmem_addr(tb, 128), v);
-    tmem_wait_ld();
-    y[0] = v[0] + s.b3[0];
-    y[1] = v[1] + s.b3[1];
+    y[0] = y0;
+    y[1] = y1;
   }
   fence_before();
   return true;
 }
 
-__device__ __forceinline__ void put_inputs(FwdSmem& s, int r, const float* in4, bool valid) {
-  float v[8] = {0, 0, 0, 0, 1.f, 0, 0, 0};
-  if (valid) { v[0] = in4[0]; v[1] = in4[1]; v[2] = in4[2]; v[3] = in4[3]; }
-  else { v[4] = 0.f; }
+// Input row r: hi(x) (cols 0-3), 1 (col 4), lo(x) (5-8), hi(x) (9-12), 0.
+template <class S>
+__device__ __forceinline__ void put_inputs(S& s, int r, const float* in4, bool valid) {
+  float v[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = 0.f;
+  if (valid) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float hi = __bfloat162float(__float2bfloat16_rn(in4[i]));
+      v[i] = hi;
+      v[5 + i] = in4[i] - hi;
+      v[9 + i] = hi;
+    }
+    v[4] = 1.f;
+  }
   put8(s.x, r, 0, 16, v);
-  float z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  put8(s.x, r, 8, 16, z);
+  put8(s.x, r, 8, 16, v + 8);
 }
 
 // Inference over n samples: out[i] = MLP(in[i]).  128 threads per CTA.
-__global__ void __launch_bounds__(TILE) forward_kernel(const float* __restrict__ in, float* __restrict__ out,
-                                                        long long n, const __nv_bfloat16* __restrict__ pk,
-                                                        const float* __restrict__ prm, int* err) {
+__global__ void __launch_bounds__(TILE, 4) forward_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                                           long long n, const __nv_bfloat16* __restrict__ pk,
+                                                           const float* __restrict__ prm, int* err) {
   extern __shared__ __align__(128) unsigned char smraw[];
-  FwdSmem& s = *reinterpret_cast<FwdSmem*>(smraw);
+  InfSmem& s = *reinterpret_cast<InfSmem*>(smraw);
   const int t = threadIdx.x;
-  load_weights(s, pk, prm);
+  load_weights(s, pk, prm, PK_INF);
   if (t == 0) { mbar_init(&s.bar, 1); s.err = 0; }
-  if (t < 32) tmem_alloc(&s.tmem, 256);
+  if (t < 32) tmem_alloc(&s.tmem, 128);
   fence_before();
   __syncthreads();
   fence_after();
@@ -410,13 +460,13 @@ __global__ void __launch_bounds__(TILE) forward_kernel(const float* __restrict__
     }
     put_inputs(s, t, in4, valid);
     float y[2];
-    if (!forward_tile(s, phase, y)) { s.err = 1; break; }
+    if (!forward_tile<64, false>(s, nullptr, phase, y)) { s.err = 1; break; }
     if (valid) { out[2 * i] = y[0]; out[2 * i + 1] = y[1]; }
   }
   fence_before();
   __syncthreads();
   fence_after();
-  if (t < 32) tmem_free(s.tmem, 256);
+  if (t < 32) tmem_free(s.tmem, 128);
   if (t == 0 && s.err) atomicAdd(err, 1);
 }
 
@@ -425,7 +475,7 @@ __global__ void __launch_bounds__(TILE) forward_kernel(const float* __restrict__
 // `tiles` consecutive tiles per CTA; the weight gradients accumulate in TMEM
 // across the CTA's tiles and are added to the global FP32 gradient at the end.
 //
-// TMEM columns: [0,64) z1, [64,128) z2, [128,144) y, [144,160) free,
+// TMEM columns: [0,64) z1, [64,128) z2, [128,160) free,
 // [160,224) dH2 then dH1, [256,272) dW3 (rows = hidden2, row 64 = db3),
 // [288,352) dW2 (rows = hidden1, row 64 = db2), [352,368) dW1^T
 // (rows = hidden1, column 4 = db1).  512 columns.
@@ -438,7 +488,7 @@ __global__ void __launch_bounds__(TILE) train_kernel(const float* __restrict__ i
   FwdSmem& s = *reinterpret_cast<FwdSmem*>(smraw);
   BwdSmem& b = *reinterpret_cast<BwdSmem*>(smraw + ((sizeof(FwdSmem) + 127) / 128) * 128);
   const int t = threadIdx.x;
-  load_weights(s, pk, prm);
+  load_weights(s, pk, prm, PK_N);
   if (t == 0) { mbar_init(&s.bar, 1); s.err = 0; }
   if (t < 32) tmem_alloc(&s.tmem, 512);
   pad_row(s.h1, t);
@@ -473,7 +523,7 @@ __global__ void __launch_bounds__(TILE) train_kernel(const float* __restrict__ i
     }
     put_inputs(s, t, in4, valid);
     float y[2];
-    if (!forward_tile(s, phase, y)) { ok = false; break; }
+    if (!forward_tile<128, true>(s, s.h2, phase, y)) { ok = false; break; }
     // loss = sum (y - t)^2 * gscale ; dL/dy = 2 (y - t) * gscale
     float dy[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (valid) {
@@ -629,19 +679,27 @@ __device__ __forceinline__ void cm_rc(int o, int C, int* r, int* c) {
   *c = (cb % (C >> 3)) * 8 + (w & 7);
 }
 
+__device__ __forceinline__ float bf16_hi(float a) { return __bfloat162float(__float2bfloat16_rn(a)); }
+
 __global__ void pack_kernel(const float* __restrict__ prm, __nv_bfloat16* __restrict__ pk) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < PK_N; e += gridDim.x * blockDim.x) {
     float v = 0.f;
     int n, k;
-    if (e < PK_W2B) {  // W1B [64][16]: (n,k) = W1[k][n]
+    if (e < PK_W2B) {  // W1B [64][16]
       cm_rc(e - PK_W1B, 16, &n, &k);
-      v = k < NIN ? prm[OFF_W1 + k * NH + n] : 0.f;
-    } else if (e < PK_W3B) {  // W2B [64][64]: (n,k) = W2[k][n]
+      if (k < NIN) v = prm[OFF_W1 + k * NH + n];
+      else if (k >= 5 && k < 5 + NIN) v = prm[OFF_W1 + (k - 5) * NH + n];
+      else if (k >= 9 && k < 9 + NIN) {
+        const float a = prm[OFF_W1 + (k - 9) * NH + n];
+        v = a - bf16_hi(a);
+      }
+    } else if (e < PK_W2L) {  // W2B [64][64]: (n,k) = hi(W2[k][n])
       cm_rc(e - PK_W2B, 64, &n, &k);
       v = prm[OFF_W2 + k * NH + n];
-    } else if (e < PK_W3R) {  // W3B [16][64]: (n,k) = W3[k][n]
-      cm_rc(e - PK_W3B, 64, &n, &k);
-      v = n < NOUT ? prm[OFF_W3 + k * NOUT + n] : 0.f;
+    } else if (e < PK_W3R) {  // W2L [64][64]: (n,k) = lo(W2[k][n])
+      cm_rc(e - PK_W2L, 64, &n, &k);
+      const float a = prm[OFF_W2 + k * NH + n];
+      v = a - bf16_hi(a);
     } else if (e < PK_W2R) {  // W3R [64][16]: (n,k) = W3[n][k]
       cm_rc(e - PK_W3R, 16, &n, &k);
       v = k < NOUT ? prm[OFF_W3 + n * NOUT + k] : 0.f;
@@ -651,6 +709,117 @@ __global__ void pack_kernel(const float* __restrict__ prm, __nv_bfloat16* __rest
     }
     pk[e] = __float2bfloat16_rn(v);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Fused source step with the surrogate: updatePrims, then for every cell
+// either the MLP's (delta x_HII, delta log10 T) -- when the cell lies in the
+// trust box and in a trusted bin of the table -- or the plain FP64
+// hrate + cooling_h step, then the CFL minimum.  Tiles of 128 cells of one
+// block; the MMA work of a tile is uniform, the fallback is per cell.
+struct SurrParams {
+  double* __restrict__ u;
+  const DevBlock* __restrict__ blocks;
+  const int32_t* __restrict__ work;
+  int nwork;
+  DevCtl* ctl;
+  PhysParams ph;
+  const __nv_bfloat16* __restrict__ pk;
+  const float* __restrict__ prm;
+  const uint8_t* __restrict__ trust;
+  int do_dt;
+  int* err;
+};
+
+template <int NEQ>
+__global__ void __launch_bounds__(TILE, 4) surrogate_source_kernel(SurrParams P) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  InfSmem& s = *reinterpret_cast<InfSmem*>(smraw);
+  const int t = threadIdx.x;
+  const PhysParams& ph = P.ph;
+  load_weights(s, P.pk, P.prm, PK_INF);
+  if (t == 0) { mbar_init(&s.bar, 1); s.err = 0; }
+  if (t < 32) tmem_alloc(&s.tmem, 128);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  uint32_t phase = 0;
+  const double dts = P.ctl->dt * ph.t_sc;
+  const float lgd = log10f((float)(dts / 3.155673600e+7));
+  const bool dt_in = lgd >= (float)Box::LD_LO && lgd <= (float)Box::LD_HI;
+  const double inv_mu0 = 1.0 / ph.mu0;
+  const double cf_min = 1.0 - ph.cooling_limit;
+  double dtl = 1.0e300, mloss = 0.0;
+  unsigned nsur = 0, nplain = 0;
+  const long long ntiles = (long long)P.nwork * (BCELLS / TILE);
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int slot = P.work[tile / (BCELLS / TILE)];
+    const int c = (int)(tile % (BCELLS / TILE)) * TILE + t;
+    const size_t o = ((size_t)slot * NEQ) * BCELLS + c;
+    double u[NEQ], p[NEQ];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) u[e] = P.u[o + (size_t)e * BCELLS];
+    flow2prim<NEQ, false>(u, p, ph.cv);
+    // gate: inside the training box and in a trusted bin (FP32 logs)
+    const double dh = p[0] * inv_mu0;
+    const double y0 = p[5] / dh;
+    const double T0 = calc_temp<5>(p, ph);
+    const float lgn = log10f((float)dh), lgT = log10f((float)T0), x0 = (float)(1.0 - y0);
+    bool use = dt_in && lgn >= (float)Box::LN_LO && lgn <= (float)Box::LN_HI && lgT >= (float)Box::LT_LO &&
+               lgT <= (float)Box::LT_HI && x0 >= 0.f && x0 <= 1.f;
+    if (use) {
+      const int bn = min(TRUST_ND - 1, max(0, (int)floorf((lgn + lgd - (float)TRUST_ND_LO) * (float)(1.0 / TRUST_ND_W))));
+      const int bt = min(TRUST_T - 1, max(0, (int)floorf((lgT - (float)TRUST_T_LO) * (float)(1.0 / TRUST_T_W))));
+      const int bx = min(TRUST_X - 1, (int)(x0 * TRUST_X));
+      use = P.trust[(bn * TRUST_T + bt) * TRUST_X + bx] != 0;
+    }
+    if (__syncthreads_or(use)) {  // the tile's MMAs run only if some cell uses them
+      float in4[4];
+      normalise(lgn, lgT, x0, lgd, in4);
+      put_inputs(s, t, in4, use);
+      float y[2];
+      if (!forward_tile<64, false>(s, nullptr, phase, y)) { s.err = 1; break; }
+      if (use) {
+        double y1 = 1.0 - ((double)x0 + (double)y[0] * Box::SCALE_X);
+        y1 = dmin(y1, 1.0 - 1.e-4);
+        y1 = dmax(y1, 0.0);
+        const double cf = (double)exp10f(y[1] * (float)Box::SCALE_C);
+        mloss = dmax(mloss, 1.0 - cf);
+        p[4] *= dmin(1.0, dmax(cf, cf_min));
+        p[5] = p[0] * y1 * inv_mu0;
+        u[5] = p[5];
+        const double EK = 0.5 * p[0] * (p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
+        u[4] = EK + ph.cv * p[4];
+        ++nsur;
+      }
+    }
+    if (!use) {
+      h_cool_step<5>(u, p, dts, ph, &mloss);
+      ++nplain;
+    }
+    P.u[o + 4 * (size_t)BCELLS] = u[4];
+    P.u[o + 5 * (size_t)BCELLS] = u[5];
+    if (P.do_dt) dtl = dmin(dtl, cell_dt<NEQ, false>(p, P.blocks[slot], ph.gamma));
+  }
+  if (P.do_dt) {
+    double v = dtl;
+    for (int k = 16; k > 0; k >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, k));
+    if ((t & 31) == 0) atomic_min_pos(&P.ctl->dtmin_bits, v);
+  }
+  double mm = mloss;
+  for (int k = 16; k > 0; k >>= 1) mm = fmax(mm, __shfl_xor_sync(0xffffffffu, mm, k));
+  if ((t & 31) == 0 && mm > 0.0) atomic_max_pos(&P.ctl->maxloss_bits, mm);
+  nsur = __reduce_add_sync(0xffffffffu, nsur);
+  nplain = __reduce_add_sync(0xffffffffu, nplain);
+  if ((t & 31) == 0) {
+    if (nsur) atomicAdd(&P.ctl->sur[0], (unsigned long long)nsur);
+    if (nplain) atomicAdd(&P.ctl->sur[1], (unsigned long long)nplain);
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (t < 32) tmem_free(s.tmem, 128);
+  if (t == 0 && s.err) atomicAdd(P.err, 1);
 }
 
 }  // namespace mlp
@@ -673,6 +842,26 @@ struct wx_mlp {
   long long step = 0;
   int nsm = 148;
 };
+
+namespace wx {
+
+cudaError_t launch_surrogate_source(const SurrLaunch& L, cudaStream_t s) {
+  SurrParams P{L.u, L.blocks, L.work, L.nwork, L.ctl, L.ph, L.mlp->pk, L.mlp->prm, L.trust, L.do_dt, L.mlp->err};
+  const long long ntiles = (long long)L.nwork * (BCELLS / TILE);
+  const int grid = (int)std::min<long long>(ntiles, 4LL * L.nsm);
+  if (L.neq == 6) {
+    cudaFuncSetAttribute(surrogate_source_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INF_SMEM);
+    surrogate_source_kernel<6><<<grid, TILE, INF_SMEM, s>>>(P);
+  } else if (L.neq == 7) {
+    cudaFuncSetAttribute(surrogate_source_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INF_SMEM);
+    surrogate_source_kernel<7><<<grid, TILE, INF_SMEM, s>>>(P);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace wx
 
 namespace {
 
@@ -742,7 +931,7 @@ int wx3d_mlp_create(uint64_t seed, wx_mlp** out) {
   cudaMemset(w->err, 0, 4);
   pack_kernel<<<(PK_N + 255) / 256, 256>>>(w->prm, w->pk);
   if (cudaDeviceSynchronize() != cudaSuccess) { delete w; return WX_ERR_CUDA; }
-  cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FwdSmem));
+  cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INF_SMEM);
   cudaFuncSetAttribute(train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem());
   *out = w;
   return WX_OK;
@@ -771,8 +960,8 @@ int wx3d_mlp_set_params(wx_mlp* w, const float* host) {
 }
 
 // Training / evaluation samples from the plain FP64 integrator.  d_in
-// [n][4] normalised inputs, d_tgt [n][2] targets (delta x_HII, delta
-// log10 T / 0.5), d_raw [n][4] (n_H, T, x_HII, dt in s) or NULL.
+// [n][4] normalised inputs, d_tgt [n][2] targets (delta x_HII / 0.125,
+// log10(P1/P0) / log10 2), d_raw [n][4] (n_H, T, x_HII, dt in s) or NULL.
 int wx3d_mlp_samples(const wx_config* cfg, int64_t n, uint64_t seed, float* d_in, float* d_tgt, double* d_raw,
                      void* stream) {
   if (!cfg || n <= 0 || !d_in || !d_tgt) return WX_ERR_INVALID_ARG;
@@ -786,9 +975,9 @@ int wx3d_mlp_samples(const wx_config* cfg, int64_t n, uint64_t seed, float* d_in
 int wx3d_mlp_forward(wx_mlp* w, int64_t n, const float* d_in, float* d_out, void* stream) {
   if (!w || n <= 0 || !d_in || !d_out) return WX_ERR_INVALID_ARG;
   const long long ntiles = (n + TILE - 1) / TILE;
-  const int grid = (int)std::min<long long>(ntiles, 2LL * w->nsm);
+  const int grid = (int)std::min<long long>(ntiles, 4LL * w->nsm);
   cudaMemsetAsync(w->err, 0, 4, (cudaStream_t)stream);
-  forward_kernel<<<grid, TILE, sizeof(FwdSmem), (cudaStream_t)stream>>>(d_in, d_out, n, w->pk, w->prm, w->err);
+  forward_kernel<<<grid, TILE, INF_SMEM, (cudaStream_t)stream>>>(d_in, d_out, n, w->pk, w->prm, w->err);
   if (cudaGetLastError() != cudaSuccess) return WX_ERR_CUDA;
   if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return WX_ERR_CUDA;
   return mlp_check(w);

@@ -112,4 +112,36 @@ __device__ __forceinline__ double find_coef(const double* __restrict__ lt, const
   return pow(10., (C1 - C0) / (T1 - T0) * (logT - T0) + C0);
 }
 
+// One plain step of updateNeutralFraction then apply_cooling_h_neq for a cell
+// (hrate.f90:101-140, cooling_h.f90:175-246) on its conserved u and
+// primitive p vectors -- the arithmetic of source_kernel's fused H_RATE +
+// COOL_H path.  FP is the index of the neutral-H passive scalar.
+template <int FP>
+__device__ __forceinline__ void h_cool_step(double* u, double* p, double dts, const PhysParams& ph, double* mloss) {
+  {
+    const double T = calc_temp<FP>(p, ph);
+    const double dh = p[0] / ph.mu0;
+    const double y0 = p[FP] / dh;
+    const double y1 = h_rate_y1(T, dh, y0, dts);
+    p[FP] = p[0] * y1 / ph.mu0;
+  }
+  const double dh = p[0] / ph.mu0;
+  const double dh0 = p[FP];
+  const double y0 = ph.mu0 * u[FP] / u[0];
+  u[FP] = p[FP];
+  const double Temp = calc_temp<FP>(p, ph);
+  if (Temp > 1.e4) {
+    const double L0 = aloss_h(y0, dh, dh0, Temp);
+    const double ce = (2.0 * L0) / (3.0 * KB * dh * Temp);
+    const double T1 = 10.0 + (Temp - 10.0) * exp(-ce * dts);
+    double cf = T1 / Temp;
+    *mloss = dmax(*mloss, 1.0 - cf);
+    if (cf < 1.0 - ph.cooling_limit) cf = 1.0 - ph.cooling_limit;
+    if (Temp * cf < 10.0) cf = 10.0 / Temp;
+    p[4] = p[4] * cf;
+    const double EK = 0.5 * p[0] * (p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
+    u[4] = EK + ph.cv * p[4];
+  }
+}
+
 }  // namespace wx

@@ -50,7 +50,9 @@ __global__ void __launch_bounds__(256) source_kernel(SrcParams P) {
         flow2prim<NEQ, MHD>(u, p, ph.cv);
       }
       constexpr int fp = FP;
-      if (HAS_PAS && do_hrate && ph.eos == WX_EOS_H_RATE) {  // hrate.f90:101-140
+      if (HAS_PAS && do_hrate && do_cool && ph.eos == WX_EOS_H_RATE && ph.cooling == WX_COOL_H) {
+        h_cool_step<FP>(u, p, dts, ph, &mloss);  // hrate.f90:101-140 then cooling_h.f90:175-246
+      } else if (HAS_PAS && do_hrate && ph.eos == WX_EOS_H_RATE) {  // hrate.f90:101-140
         const double T = calc_temp<FP>(p, ph);
         const double dh = p[0] / ph.mu0;
         const double y0 = p[fp] / dh;
@@ -58,7 +60,9 @@ __global__ void __launch_bounds__(256) source_kernel(SrcParams P) {
         p[fp] = p[0] * y1 / ph.mu0;
         if (ph.cooling != WX_COOL_H) u[fp] = p[fp];
       }
-      if (do_cool && ph.cooling == WX_COOL_TABLE && P.ncool >= 2) {  // cooling.f90:303-369
+      if (HAS_PAS && do_hrate && do_cool && ph.eos == WX_EOS_H_RATE && ph.cooling == WX_COOL_H) {
+        // done above
+      } else if (do_cool && ph.cooling == WX_COOL_TABLE && P.ncool >= 2) {  // cooling.f90:303-369
         const double temp = calc_temp<FP>(p, ph);
         const double logT = log10(temp);
         if (logT >= P.cool_lt[0]) {

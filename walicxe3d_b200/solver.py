@@ -54,6 +54,10 @@ class Walicxe3D:
         if self.ctx:
             self.lib.wx3d_finalize(self.ctx)
             self.ctx = None
+        sur = getattr(self, "_surrogate", None)
+        if sur is not None:
+            sur.close()
+            self._surrogate = None
 
     def __enter__(self):
         return self
@@ -138,6 +142,9 @@ class Walicxe3D:
         self._chk(self.lib.wx3d_get_status(self.ctx, ctypes.byref(s)), "wx3d_get_status")
         return s
 
+    def reset_status(self):
+        self._chk(self.lib.wx3d_reset_status(self.ctx), "wx3d_reset_status")
+
     # -- the reference's hot-path subroutines ---------------------------------
     def get_timestep(self) -> float:
         dt = ctypes.c_double()
@@ -163,6 +170,13 @@ class Walicxe3D:
     def cooling(self) -> float:
         m = ctypes.c_double()
         self._chk(self.lib.wx3d_cooling(self.ctx, ctypes.byref(m)), "wx3d_cooling")
+        return m.value
+
+    def sources(self) -> float:
+        """updatePrims + updateNeutralFraction + cooling in one fused pass
+        (the surrogate's, when attached); returns maxloss."""
+        m = ctypes.c_double()
+        self._chk(self.lib.wx3d_sources(self.ctx, ctypes.byref(m)), "wx3d_sources")
         return m.value
 
     def set_cooltable(self, logT, b):
@@ -196,6 +210,25 @@ class Walicxe3D:
     def coarsen(self, child_slots, father_slot: int):
         ch, p = _i32(child_slots)
         self._chk(self.lib.wx3d_coarsen(self.ctx, p, int(father_slot)), "wx3d_coarsen")
+
+    def attach_surrogate(self, params=None, trust=None):
+        """Source steps of step()/run() use the trained MLP where its trust
+        table allows and the plain integrator elsewhere.  Defaults to the
+        network shipped in walicxe3d_b200/data."""
+        from .surrogate import Surrogate
+        if params is None or trust is None:
+            from .train_surrogate import load
+            p0, t0 = load()
+            params = p0 if params is None else params
+            trust = t0 if trust is None else trust
+        self._surrogate = Surrogate()
+        self._surrogate.params = params
+        tb = np.ascontiguousarray(trust, dtype=np.uint8).ravel()
+        self._chk(self.lib.wx3d_set_surrogate(self.ctx, self._surrogate.h, tb.ctypes.data_as(ctypes.c_void_p),
+                                              tb.size, 1), "wx3d_set_surrogate")
+
+    def detach_surrogate(self):
+        self._chk(self.lib.wx3d_set_surrogate(self.ctx, None, None, 0, 0), "wx3d_set_surrogate")
 
     def set_timing(self, on: bool):
         self._chk(self.lib.wx3d_set_timing(self.ctx, int(bool(on))), "wx3d_set_timing")

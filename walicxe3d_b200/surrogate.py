@@ -1,8 +1,9 @@
 """Learned surrogate of the hydrogen-rate + cooling_h update.
 
 Host mirror of the wx3d_mlp_* entry points (include/wx3d.h): a 4-64-64-2
-SiLU MLP, BF16 weights with FP32 accumulation, whose forward, backward and
-weight-gradient products run as tcgen05 tensor-core MMAs.  Device buffers are
+SiLU MLP, BF16 operands with FP32 accumulation, whose hidden layers (split
+into BF16 head and tail in the forward pass), backward and weight-gradient
+products run as tcgen05 tensor-core MMAs; the output layer is FP32.  Device buffers are
 torch CUDA tensors (plumbing only); every computation runs in libwx3d.so.
 """
 from __future__ import annotations
@@ -21,7 +22,10 @@ NPARAM = NIN * NH + NH + NH * NH + NH + NH * NOUT + NOUT
 LOG_N = (-3.0, 4.0)      # log10 n_H [cm^-3]
 LOG_T = (2.0, 8.0)       # log10 T [K]
 LOG_DT = (-2.0, 3.0)     # log10 dt [yr]
-SCALE_T = 0.5            # the second output is delta log10 T / SCALE_T
+# Outputs: delta x_HII / SCALE_X and log10(cf) / SCALE_C, where the cooling
+# factor cf = P1/P0 is the pressure ratio of the step
+SCALE_X = 0.125
+SCALE_C = 0.30102999566398120
 
 
 def _vp(t):
