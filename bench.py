@@ -38,7 +38,7 @@ WORKLOADS = {
     "sedov256": dict(desc="Sedov blast 16^3 root blocks of 16^3 (256^3 cells), single level, FP64 HLLC+minmod"),
     "sedov64": dict(desc="Sedov blast 4^3 root blocks of 16^3 (64^3 cells), single level, FP64 HLLC+minmod"),
     "brio-wu": dict(desc="Brio-Wu MHD shock tube 256x16x16 cells, FP64 HLLD+minmod, 8-wave source"),
-    "snr-h": dict(desc="radiative SNR, H-rate EOS + COOL_H, 4^3 roots, 3 levels, FP64 HLLC+minmod"),
+    "snr-h": dict(desc="radiative SNR, H-rate EOS + COOL_H, 8^3 roots, 4 levels (4,712 blocks), FP64 HLLC+minmod"),
 }
 
 
@@ -53,7 +53,7 @@ def build_problem(name: str):
     if name == "brio-wu":
         return problems.brio_wu(16)
     if name == "snr-h":
-        return problems.snr_h(nroot=4, maxlev=3)
+        return problems.snr_h(nroot=8, maxlev=4)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -191,6 +191,8 @@ def main():
     ap.add_argument("--workload", default="blast-amr", choices=sorted(WORKLOADS))
     ap.add_argument("--zsplit", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--surrogate", action="store_true",
+                    help="attach the trained hrate + cooling_h surrogate (EOS_H_RATE + COOL_H workloads)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -229,6 +231,8 @@ def main():
     else:
         from walicxe3d_b200.autotune import tune
         tuned = tune(w, prob, cache=None, reps=2)
+    if args.surrogate:
+        w.attach_surrogate()
     w.set_timing(True)
 
     # --- warm-up (graph capture happens here) ---
@@ -240,6 +244,7 @@ def main():
     sampler.start()
     time.sleep(0.3)
     k0 = w.kernels_launched
+    w.reset_status()
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
@@ -251,6 +256,8 @@ def main():
     ms = e0.elapsed_time(e1)
     launches = w.kernels_launched - k0
     kt_ms, kt_n = w.kernel_times()
+    wst = w.status()
+    sur_cells, fb_cells = int(wst.surrogate_cells), int(wst.fallback_cells)
     clocks = sampler.stop()
     st = w.state
     if dist is not None:
@@ -334,6 +341,8 @@ def main():
                     "note": "timed: upload of the state from pinned host memory, K wx3d_step calls (each "
                             "returns time/dt/status to the host), download of the final state"},
             "gpu_launches": launches,
+            "surrogate": ({"attached": True, "surrogate_cells": sur_cells, "fallback_cells": fb_cells,
+                           "share": sur_cells / max(1, sur_cells + fb_cells)} if args.surrogate else None),
             "clocks": clocks,
             "cpu_baseline": cpu,
             "final_state": {"time": st.time, "dt": st.dt, "it": st.it},

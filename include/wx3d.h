@@ -309,9 +309,9 @@ int wx3d_mlp_train(wx_mlp* mlp, int64_t n, const float* d_in, const float* d_tar
 /* Attaches (enable = 1) the surrogate to a context whose config is
  * EOS_H_RATE + COOL_H: the source step of wx3d_step / wx3d_run then uses the
  * MLP for the cells in the trust box whose bin of `trust` is non-zero, and
- * the plain integrator elsewhere.  trust[24][24][4] (nbytes = 2304) bins
- * log10(n_H dt/yr) in [-5,7) by 0.5, log10 T in [2,8) by 0.25 and x_HII in
- * quarters.  enable = 0 detaches it. */
+ * the plain integrator elsewhere.  trust[48][48][8] (nbytes = 18432) bins
+ * log10(n_H dt/yr) in [-5,7) by 0.25, log10 T in [2,8) by 0.125 and x_HII
+ * in eighths.  enable = 0 detaches it. */
 int wx3d_set_surrogate(wx_ctx* ctx, wx_mlp* mlp, const uint8_t* trust, int32_t nbytes, int32_t enable);
 
 /* Human-readable text of a status code and of the context's last error. */

@@ -46,7 +46,9 @@ def test_gradient_matches_fp64_reference():
     le, ge = mlp_ref.loss_grad(p.astype(np.float64), x.astype(np.float64), t.astype(np.float64), quant=False)
     assert loss == pytest.approx(lq, rel=1e-3)
     # same rounding points: agreement to FP32 accumulation order
-    assert np.linalg.norm(g - gq) <= 1e-3 * np.linalg.norm(gq)
+    # (the SiLU uses the hardware tanh approximation, relative error ~2^-11,
+    # which the FP64 reference does not emulate)
+    assert np.linalg.norm(g - gq) <= 5e-3 * np.linalg.norm(gq)
     # against the exact FP64 gradient: BF16 operands only
     cos = g @ ge / (np.linalg.norm(g) * np.linalg.norm(ge))
     assert cos >= 0.999

@@ -11,7 +11,7 @@ from walicxe3d_b200 import config as C
 pytestmark = pytest.mark.gpu
 
 MU0 = 1.3
-TRUST_SHAPE = (24, 24, 4)
+TRUST_SHAPE = (48, 48, 8)
 
 
 def _cfg(nblocks):

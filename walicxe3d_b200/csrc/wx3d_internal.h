@@ -11,9 +11,9 @@ struct wx_mlp;
 namespace wx {
 
 // Trust table of the surrogate: bins of log10(n_H * dt/yr), log10 T, x_HII.
-constexpr int TRUST_ND = 24, TRUST_T = 24, TRUST_X = 4;
-constexpr double TRUST_ND_LO = -5.0, TRUST_ND_W = 0.5;
-constexpr double TRUST_T_LO = 2.0, TRUST_T_W = 0.25;
+constexpr int TRUST_ND = 48, TRUST_T = 48, TRUST_X = 8;
+constexpr double TRUST_ND_LO = -5.0, TRUST_ND_W = 0.25;
+constexpr double TRUST_T_LO = 2.0, TRUST_T_W = 0.125;
 constexpr int TRUST_BYTES = TRUST_ND * TRUST_T * TRUST_X;
 
 struct SurrLaunch {

@@ -186,9 +186,19 @@ __device__ __forceinline__ void put8_split(__nv_bfloat16* hi, int C, __nv_bfloat
   *reinterpret_cast<uint4*>(lo + cm_off(r, c, CL)) = *reinterpret_cast<const uint4*>(ql);
 }
 
-__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+// SiLU(z) = z sigma(z) with sigma(z) = (1 + tanh(z/2)) / 2: one tanh.approx
+// (a single SFU operation, relative error about 2^-11) per activation.
+__device__ __forceinline__ float tanh_approx(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float silu(float z) {
+  const float h = 0.5f * z;
+  return fmaf(h, tanh_approx(h), h);
+}
 __device__ __forceinline__ float dsilu(float z) {
-  const float s = __fdividef(1.0f, 1.0f + __expf(-z));
+  const float s = fmaf(0.5f, tanh_approx(0.5f * z), 0.5f);
   return s * (1.0f + z * (1.0f - s));
 }
 
@@ -283,20 +293,28 @@ struct __align__(128) FwdSmem {
 };
 
 struct __align__(128) InfSmem {
-  __nv_bfloat16 x[TILE * 16];     // [128][16]  inputs hi(x), 1, lo(x), hi(x)
-  __nv_bfloat16 h1[TILE * 64];    // [128][64]  hi(SiLU(z1))
+  // The inputs are dead once the layer-1 MMA has completed, before the
+  // first hidden layer is written, and the next tile's inputs are written
+  // after the layer-2 MMA has completed: the two share their bytes.
+  union {
+    __nv_bfloat16 x[TILE * 16];   // [128][16]  inputs hi(x), 1, lo(x), hi(x)
+    __nv_bfloat16 h1[TILE * 64];  // [128][64]  hi(SiLU(z1))
+  };
   __nv_bfloat16 h1lo[TILE * 64];  // [128][64]  lo(SiLU(z1))
   __nv_bfloat16 w[PK_INF];        // W1B, W2B, W2L
   float b1[NH], b2[NH], w3[NH * NOUT], b3[16];
+  int queue[2 * TILE];            // fallback cells of the fused source kernel
+  int qn;
   uint64_t bar;
   uint32_t tmem;
   int err;
 };
 // Inference CTAs allocate 128 TMEM columns; the dynamic shared memory of an
-// inference launch is padded so that at most four CTAs share an SM and
-// their allocations (4 x 128 of 512 columns) never wait on each other.
+// inference launch is padded so that at most four CTAs share an SM (five
+// would need more than the 228 KB of an SM) and their allocations
+// (4 x 128 of 512 columns) never wait on each other.
 constexpr size_t INF_SMEM = 56 * 1024;
-static_assert(sizeof(InfSmem) <= INF_SMEM, "inference shared memory");
+static_assert(sizeof(InfSmem) <= INF_SMEM && 5 * (INF_SMEM + 1024) > 228 * 1024, "inference shared memory");
 
 struct __align__(128) BwdSmem {
   __nv_bfloat16 dy[TILE * 16];    // [128][16]  output gradient (cols 0,1)
@@ -731,14 +749,36 @@ struct SurrParams {
   int* err;
 };
 
+// Plain FP64 hrate + cooling_h step of one cell (the fallback), with its
+// store and its CFL contribution.
+template <int NEQ>
+__device__ __forceinline__ void fallback_cell(const SurrParams& P, int id, double dts, double& dtl, double& mloss) {
+  const int slot = id >> 12, c = id & (BCELLS - 1);
+  const size_t o = ((size_t)slot * NEQ) * BCELLS + c;
+  double u[NEQ], p[NEQ];
+#pragma unroll
+  for (int e = 0; e < NEQ; ++e) u[e] = P.u[o + (size_t)e * BCELLS];
+  flow2prim<NEQ, false>(u, p, P.ph.cv);
+  h_cool_step<5>(u, p, dts, P.ph, &mloss);
+  P.u[o + 4 * (size_t)BCELLS] = u[4];
+  P.u[o + 5 * (size_t)BCELLS] = u[5];
+  if (P.do_dt) dtl = dmin(dtl, cell_dt<NEQ, false>(p, P.blocks[slot], P.ph.gamma));
+}
+
+// Cells that fall back are queued in shared memory (id = slot * 4096 + cell)
+// and integrated 128 at a time, so a warp runs the plain integrator only
+// for a full set of fallback cells, not for each of its tiles that holds
+// one.
 template <int NEQ>
 __global__ void __launch_bounds__(TILE, 4) surrogate_source_kernel(SurrParams P) {
   extern __shared__ __align__(128) unsigned char smraw[];
   InfSmem& s = *reinterpret_cast<InfSmem*>(smraw);
-  const int t = threadIdx.x;
+  int* queue = s.queue;
+  int& qn = s.qn;
+  const int t = threadIdx.x, lane = t & 31;
   const PhysParams& ph = P.ph;
   load_weights(s, P.pk, P.prm, PK_INF);
-  if (t == 0) { mbar_init(&s.bar, 1); s.err = 0; }
+  if (t == 0) { mbar_init(&s.bar, 1); s.err = 0; qn = 0; }
   if (t < 32) tmem_alloc(&s.tmem, 128);
   fence_before();
   __syncthreads();
@@ -773,6 +813,14 @@ __global__ void __launch_bounds__(TILE, 4) surrogate_source_kernel(SurrParams P)
       const int bx = min(TRUST_X - 1, (int)(x0 * TRUST_X));
       use = P.trust[(bn * TRUST_T + bt) * TRUST_X + bx] != 0;
     }
+    // queue the fallback cells (warp-aggregated)
+    {
+      const unsigned fb = __ballot_sync(0xffffffffu, !use);
+      int base = 0;
+      if (lane == 0 && fb) base = atomicAdd(&qn, __popc(fb));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (!use) queue[base + __popc(fb & ((1u << lane) - 1u))] = (slot << 12) | c;
+    }
     if (__syncthreads_or(use)) {  // the tile's MMAs run only if some cell uses them
       float in4[4];
       normalise(lgn, lgT, x0, lgd, in4);
@@ -787,31 +835,42 @@ __global__ void __launch_bounds__(TILE, 4) surrogate_source_kernel(SurrParams P)
         mloss = dmax(mloss, 1.0 - cf);
         p[4] *= dmin(1.0, dmax(cf, cf_min));
         p[5] = p[0] * y1 * inv_mu0;
-        u[5] = p[5];
         const double EK = 0.5 * p[0] * (p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
-        u[4] = EK + ph.cv * p[4];
+        P.u[o + 4 * (size_t)BCELLS] = EK + ph.cv * p[4];
+        P.u[o + 5 * (size_t)BCELLS] = p[5];
+        if (P.do_dt) dtl = dmin(dtl, cell_dt<NEQ, false>(p, P.blocks[slot], ph.gamma));
         ++nsur;
       }
     }
-    if (!use) {
-      h_cool_step<5>(u, p, dts, ph, &mloss);
+    __syncthreads();
+    const int q = qn;
+    if (q >= TILE) {  // a full set: one queued cell per thread
+      fallback_cell<NEQ>(P, queue[q - TILE + t], dts, dtl, mloss);
+      ++nplain;
+      __syncthreads();
+      if (t == 0) qn = q - TILE;
+      __syncthreads();
+    }
+  }
+  {  // the remainder of the queue
+    __syncthreads();
+    const int q = qn;
+    if (t < q) {
+      fallback_cell<NEQ>(P, queue[t], dts, dtl, mloss);
       ++nplain;
     }
-    P.u[o + 4 * (size_t)BCELLS] = u[4];
-    P.u[o + 5 * (size_t)BCELLS] = u[5];
-    if (P.do_dt) dtl = dmin(dtl, cell_dt<NEQ, false>(p, P.blocks[slot], ph.gamma));
   }
   if (P.do_dt) {
     double v = dtl;
     for (int k = 16; k > 0; k >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, k));
-    if ((t & 31) == 0) atomic_min_pos(&P.ctl->dtmin_bits, v);
+    if (lane == 0) atomic_min_pos(&P.ctl->dtmin_bits, v);
   }
   double mm = mloss;
   for (int k = 16; k > 0; k >>= 1) mm = fmax(mm, __shfl_xor_sync(0xffffffffu, mm, k));
-  if ((t & 31) == 0 && mm > 0.0) atomic_max_pos(&P.ctl->maxloss_bits, mm);
+  if (lane == 0 && mm > 0.0) atomic_max_pos(&P.ctl->maxloss_bits, mm);
   nsur = __reduce_add_sync(0xffffffffu, nsur);
   nplain = __reduce_add_sync(0xffffffffu, nplain);
-  if ((t & 31) == 0) {
+  if (lane == 0) {
     if (nsur) atomicAdd(&P.ctl->sur[0], (unsigned long long)nsur);
     if (nplain) atomicAdd(&P.ctl->sur[1], (unsigned long long)nplain);
   }

@@ -1,6 +1,6 @@
 """Trains the hydrogen-rate + cooling_h surrogate and builds its trust table.
 
-    python -m walicxe3d_b200.train_surrogate [--n-train 20000000] [--n-test 4000000]
+    python -m walicxe3d_b200.train_surrogate [--n-train 20000000] [--n-test 8000000]
 
 Samples come from the plain FP64 integrator on the GPU (wx3d_mlp_samples:
 log-uniform n_H in [1e-3, 1e4] cm^-3, T in [1e2, 1e8] K, dt in [1e-2, 1e3] yr,
@@ -8,8 +8,8 @@ uniform x_HII); training runs the tcgen05 forward/backward kernels with Adam
 (wx3d_mlp_train).  The trained network is then judged against the plain
 integrator on a held-out set: per bin of (log10 n_H dt/yr, log10 T, x_HII)
 the largest ionisation-fraction and temperature errors decide whether the
-bin is trusted.  A second, independent set (another seed) measures the
-errors the trusted region shows on cells it has not seen.
+bin is trusted.  A second, independent set (another seed, half the size)
+measures the errors the trusted region shows on cells it has not seen.
 
 Writes ``data/surrogate_h.npz`` (params, trust table) and
 ``data/surrogate_h.json`` (loss curve, error statistics, trusted fraction)
@@ -31,10 +31,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_OUT = os.path.join(HERE, "data", "surrogate_h")
 
 # Trust table geometry (wx3d_set_surrogate): log10(n_H dt/yr) in [-5, 7) by
-# 0.5, log10 T in [2, 8) by 0.25, x_HII in quarters.
-TRUST_ND, TRUST_T, TRUST_X = 24, 24, 4
-ND_LO, ND_W = -5.0, 0.5
-T_LO, T_W = 2.0, 0.25
+# 0.25, log10 T in [2, 8) by 0.125, x_HII in eighths.
+TRUST_ND, TRUST_T, TRUST_X = 48, 48, 8
+ND_LO, ND_W = -5.0, 0.25
+T_LO, T_W = 2.0, 0.125
 
 X_TOL = 1.0e-3      # absolute ionisation-fraction error
 T_TOL = 1.0e-2      # relative temperature error
@@ -85,12 +85,19 @@ def bin_max(ex, eT, b):
     return cnt, mx, mt
 
 
-def trust_table(ex, eT, b, margin: float = 0.75, min_count: int = 64) -> np.ndarray:
-    """A bin is trusted when it holds at least min_count held-out samples
-    and its largest errors are within margin x the tolerances."""
+def trust_table(ex, eT, b, margin: float = 0.75, min_count: int = 100) -> np.ndarray:
+    """A bin is trusted when it holds at least min_count held-out samples,
+    its largest errors are within margin x the tolerances, and so are those
+    of its neighbours in log10(n_H dt) and log10 T (the trusted region is
+    eroded by one bin, where the error surface changes fastest)."""
     cnt, mx, mt = bin_max(ex, eT, b)
     ok = (cnt >= min_count) & (mx <= margin * X_TOL) & (mt <= margin * T_TOL)
-    return ok.astype(np.uint8)
+    ok3 = ok.reshape(TRUST_ND, TRUST_T, TRUST_X)
+    pad = np.pad(ok3, ((1, 1), (1, 1), (0, 0)), constant_values=True)
+    er = ok3.copy()
+    for d0, d1 in ((-1, 0), (1, 0), (0, -1), (0, 1)):
+        er &= pad[1 + d0:1 + d0 + TRUST_ND, 1 + d1:1 + d1 + TRUST_T]
+    return er.reshape(-1).astype(np.uint8)
 
 
 # (epochs, learning rate): the whole box, then two rounds on the bins the
@@ -121,7 +128,7 @@ def train(n_train: int, n_test: int, out: str, seed: int = 1, batch: int = 16384
     cfg = training_config()
     t0 = time.time()
     x, t, r = samples(cfg, n_train, seed=SEED_TRAIN, raw=True)
-    xt, tt, rt = samples(cfg, n_test, seed=SEED_TEST, raw=True)
+    xt, tt, rt = samples(cfg, 2 * n_test, seed=SEED_TEST, raw=True)
     xv, tv, rv = samples(cfg, n_test, seed=SEED_VAL, raw=True)
     t_samples = time.time() - t0
     s = Surrogate(seed=seed)
@@ -161,7 +168,8 @@ def train(n_train: int, n_test: int, out: str, seed: int = 1, batch: int = 16384
     stats = {
         "n_train": n_train,
         "n_train_focus": n_focus,
-        "n_test": n_test,
+        "n_test": 2 * n_test,
+        "n_validation": n_test,
         "schedule_all": [list(e) for e in SCHEDULE_ALL],
         "schedule_focus": [[f, [list(e) for e in sc]] for f, sc in SCHEDULE_FOCUS],
         "trust_margin": TRUST_MARGIN,
@@ -193,7 +201,7 @@ def train(n_train: int, n_test: int, out: str, seed: int = 1, batch: int = 16384
 
 
 def load(path: str = DEFAULT_OUT):
-    """(params float32[NPARAM], trust uint8[24,24,4]) of a trained surrogate."""
+    """(params float32[NPARAM], trust uint8[48,48,8]) of a trained surrogate."""
     d = np.load(path + ".npz")
     return d["params"].astype(np.float32), d["trust"].astype(np.uint8)
 
@@ -201,7 +209,7 @@ def load(path: str = DEFAULT_OUT):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--n-train", type=int, default=20_000_000)
-    ap.add_argument("--n-test", type=int, default=4_000_000)
+    ap.add_argument("--n-test", type=int, default=8_000_000)
     ap.add_argument("--batch", type=int, default=16384)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--out", default=DEFAULT_OUT)
