@@ -314,6 +314,12 @@ int wx3d_mlp_train(wx_mlp* mlp, int64_t n, const float* d_in, const float* d_tar
  * in eighths.  enable = 0 detaches it. */
 int wx3d_set_surrogate(wx_ctx* ctx, wx_mlp* mlp, const uint8_t* trust, int32_t nbytes, int32_t enable);
 
+/* Self-check of the Newton-refined reciprocal and square root that the flux
+ * kernels use in place of IEEE division and sqrt: max_ulp2[0] and [1]
+ * receive their largest distance in ulp from the device's 1/x and sqrt(x)
+ * over the n positive normal arguments host_x. */
+int wx3d_check_fast_math(int32_t n, const double* host_x, int64_t* max_ulp2);
+
 /* Human-readable text of a status code and of the context's last error. */
 const char* wx3d_error_string(int32_t code);
 int wx3d_last_error(wx_ctx* ctx, char* buf, int32_t len);

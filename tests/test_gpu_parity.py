@@ -347,3 +347,22 @@ def test_status_counts_and_zero_density_error():
     with pytest.raises(WxError) as ei:
         g.step()
     assert ei.value.code == 23
+
+
+def test_fast_reciprocal_and_sqrt_within_two_ulp():
+    """The Newton-refined reciprocal and square root of the flux kernels
+    against the device's IEEE 1/x and sqrt(x), log-uniform over 600 decades
+    plus powers of two and values next to them."""
+    import ctypes
+
+    from walicxe3d_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(12)
+    x = 10.0 ** rng.uniform(-300, 300, 1_000_000)
+    p2 = 2.0 ** np.arange(-1000, 1000, dtype=np.float64)
+    x = np.concatenate([x, p2, np.nextafter(p2, 0), np.nextafter(p2, np.inf), [1.0, 1.4, 1e-30, 1e-40]])
+    out = np.zeros(2, np.int64)
+    rc = lib.wx3d_check_fast_math(x.size, x.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                  out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+    assert rc == 0
+    assert out[0] <= 2 and out[1] <= 2, out

@@ -399,6 +399,22 @@ void invalidate_graph(wx_ctx* c) {
 
 bool ready(wx_ctx* c) { return c && c->nwork > 0; }
 
+__device__ __forceinline__ unsigned long long ulp_dist(double a, double b) {
+  const long long x = __double_as_longlong(a), y = __double_as_longlong(b);
+  return (unsigned long long)(x > y ? x - y : y - x);
+}
+
+__global__ void fast_math_check_kernel(const double* __restrict__ x, int n, unsigned long long* ulp) {
+  unsigned long long m0 = 0, m1 = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = x[i];
+    m0 = max(m0, ulp_dist(rcp_nr(v), 1.0 / v));
+    m1 = max(m1, ulp_dist(sqrt_nr(v), sqrt(v)));
+  }
+  atomicMax(&ulp[0], m0);
+  atomicMax(&ulp[1], m1);
+}
+
 }  // namespace
 
 // =============================================================================
@@ -1007,6 +1023,29 @@ int wx3d_kernel_times(wx_ctx* c, double* ms4, int32_t* count4) {
     ms4[k] += ms;
     if (count4) ++count4[k];
   }
+  return WX_OK;
+}
+
+// Largest distance in ulp of rcp_nr / sqrt_nr from the device's IEEE 1/x and
+// sqrt(x) over n host arguments.
+int wx3d_check_fast_math(int32_t n, const double* host_x, int64_t* max_ulp2) {
+  if (n <= 0 || !host_x || !max_ulp2) return WX_ERR_INVALID_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return WX_ERR_NO_DEVICE;
+  double* dx = nullptr;
+  unsigned long long* du = nullptr;
+  if (cudaMalloc(&dx, sizeof(double) * n) != cudaSuccess) return WX_ERR_CUDA;
+  if (cudaMalloc(&du, 16) != cudaSuccess) { cudaFree(dx); return WX_ERR_CUDA; }
+  cudaMemcpy(dx, host_x, sizeof(double) * n, cudaMemcpyHostToDevice);
+  cudaMemset(du, 0, 16);
+  fast_math_check_kernel<<<256, 256>>>(dx, n, du);
+  unsigned long long h[2] = {0, 0};
+  const cudaError_t e = cudaMemcpy(h, du, 16, cudaMemcpyDeviceToHost);
+  cudaFree(dx);
+  cudaFree(du);
+  if (e != cudaSuccess) return WX_ERR_CUDA;
+  max_ulp2[0] = (int64_t)h[0];
+  max_ulp2[1] = (int64_t)h[1];
   return WX_OK;
 }
 

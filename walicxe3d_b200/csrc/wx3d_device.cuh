@@ -86,13 +86,39 @@ __device__ __forceinline__ constexpr int perm(int e) {
 __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
 __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
 
+// Reciprocal and square root for the hot flux path, without the special-case
+// branches of IEEE division and sqrt.  The hardware estimates
+// rcp.approx.ftz.f64 and rsqrt.approx.ftz.f64 are refined by two
+// Newton-Raphson steps each (quadratic convergence: r <- r + r (1 - d r) for
+// 1/d, y <- y + y (1 - x y^2) / 2 for 1/sqrt(x)); the square root is then
+// x y with one Newton correction s <- s + y (x - s^2) / 2.  The results lie
+// within a few ulp of the correctly rounded ones (checked on the device by
+// wx3d_check_fast_math).  Arguments must be positive and normal: the
+// densities and pressures that reach them have passed the floors of
+// flow2prim; zero, infinite or NaN arguments give a non-finite result.
+__device__ __forceinline__ double rcp_nr(double d) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+  r = fma(r, fma(-d, r, 1.0), r);
+  r = fma(r, fma(-d, r, 1.0), r);
+  return r;
+}
+__device__ __forceinline__ double sqrt_nr(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  y = fma(0.5 * y, fma(-x * y, y, 1.0), y);
+  y = fma(0.5 * y, fma(-x * y, y, 1.0), y);
+  const double s = x * y;
+  return fma(0.5 * y, fma(-s, s, x), s);
+}
+
 // flow2prim (hydro_core.f90:323-378).  Returns istat: 0 ok, 1 pressure
 // floor, 2 density floor, -1 zero density.
 template <int NEQ, bool MHD>
 __device__ __forceinline__ int flow2prim(const double* u, double* p, double cv, double* rinv_out = nullptr) {
   int istat = 0;
   if (u[0] == 0.0) istat = -1;
-  const double rinv = 1.0 / u[0];
+  const double rinv = 1.0 / u[0];   // IEEE: u[0] may be zero or tiny here
   if (rinv_out) *rinv_out = rinv;
   p[0] = u[0];
   p[1] = u[1] * rinv;
@@ -238,7 +264,7 @@ __device__ __forceinline__ void riemann_hllc_c(const double* pL, const double* p
   const double dl = pL[0], dr = pR[0], ul = pL[1], ur = pR[1];
   const double sl = dmin(ul - cl, ur - cr);
   const double sr = dmax(ul + cl, ur + cr);
-  const double sst = (pR[4] - pL[4] + dl * ul * (sl - ul) - dr * ur * (sr - ur)) / (dl * (sl - ul) - dr * (sr - ur));
+  const double sst = (pR[4] - pL[4] + dl * ul * (sl - ul) - dr * ur * (sr - ur)) * rcp_nr(dl * (sl - ul) - dr * (sr - ur));
   const bool useL = (sl > 0.0) || (!(sr < 0.0) && (sst >= 0.0));
   double pk[NEQ];
 #pragma unroll
@@ -249,7 +275,7 @@ __device__ __forceinline__ void riemann_hllc_c(const double* pL, const double* p
     const double rinv = useL ? rl : rr;
     const double skmu = sk - pk[1];
     const double d1 = sk - sst;
-    const double inv = 1.0 / (d1 * skmu);
+    const double inv = rcp_nr(d1 * skmu);
     const double rhost = pk[0] * (skmu * skmu) * inv;          // rho (sk-u)/(sk-sst)
     const double q = pk[4] * rinv * (d1 * inv);                 // p / (rho (sk-u))
     const double E = 0.5 * pk[0] * (pk[1] * pk[1] + pk[2] * pk[2] + pk[3] * pk[3]) + cv * pk[4];
@@ -316,7 +342,7 @@ __device__ __forceinline__ void riemann_hllc(const double* pL, const double* pR,
   const double cr = sqrt(g * pR[4] / dr);
   const double sl = dmin(ul - cl, ur - cr);
   const double sr = dmax(ul + cl, ur + cr);
-  const double sst = (pR[4] - pL[4] + dl * ul * (sl - ul) - dr * ur * (sr - ur)) / (dl * (sl - ul) - dr * (sr - ur));
+  const double sst = (pR[4] - pL[4] + dl * ul * (sl - ul) - dr * ur * (sr - ur)) * rcp_nr(dl * (sl - ul) - dr * (sr - ur));
   const bool useL = (sl > 0.0) || (!(sr < 0.0) && (sst >= 0.0));
   double pk[NEQ];
 #pragma unroll

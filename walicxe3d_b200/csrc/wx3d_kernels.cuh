@@ -61,9 +61,15 @@ __device__ __forceinline__ void flush_counts(DevCtl* ctl, unsigned pf, unsigned 
 
 // One interface flux in direction DIR from ring cells c0..c3 (pointers to
 // equation 0 of cells l-1, l, r, r+1; stride HPLANE between channels).
-template <int NEQ, bool MHD, int SOLVER, int ORDER, int LIM, int DIR>
+// With CARRY (the z-interfaces, which a thread visits in order along its
+// column) the limited slope of the lower cell is the upper cell's slope of
+// the previous interface -- the limiter sees the same two differences -- and
+// is taken from `carry` instead of being evaluated again, unless `first`;
+// the upper cell's slope is left in `carry` for the next interface.
+template <int NEQ, bool MHD, int SOLVER, int ORDER, int LIM, int DIR, bool CARRY = false>
 __device__ __forceinline__ void iface_flux(const double* c0, const double* c1, const double* c2, const double* c3,
-                                           const PhysParams& ph, double* f) {
+                                           const PhysParams& ph, double* f, double* carry = nullptr,
+                                           bool first = true) {
   double pl[NEQ], pr[NEQ], fx[NEQ];
 #pragma unroll
   for (int e = 0; e < NEQ; ++e) {
@@ -75,10 +81,13 @@ __device__ __forceinline__ void iface_flux(const double* c0, const double* c1, c
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) {
       const int q = perm<DIR, MHD>(e);
-      const double pll = c0[q * HPLANE], prr = c3[q * HPLANE];
-      const double dl = pl[e] - pll, dm = pr[e] - pl[e], dr = prr - pr[e];
-      const double al = average_t<LIM>(dl, dm, ph.limiter);
+      const double prr = c3[q * HPLANE];
+      const double dm = pr[e] - pl[e], dr = prr - pr[e];
+      double al;
+      if (!CARRY || first) al = average_t<LIM>(pl[e] - c0[q * HPLANE], dm, ph.limiter);
+      else al = carry[e];
       const double ar = average_t<LIM>(dm, dr, ph.limiter);
+      if (CARRY) carry[e] = ar;
       pl[e] = pl[e] + 0.5 * al;
       pr[e] = pr[e] - 0.5 * ar;
     }
@@ -91,10 +100,10 @@ __device__ __forceinline__ void iface_flux(const double* c0, const double* c1, c
       rl = c1[(NEQ + 1) * HPLANE];
       rr = c2[(NEQ + 1) * HPLANE];
     } else {
-      rl = 1.0 / pl[0];
-      rr = 1.0 / pr[0];
-      cl = sqrt(ph.gamma * pl[4] * rl);
-      cr = sqrt(ph.gamma * pr[4] * rr);
+      rl = rcp_nr(pl[0]);
+      rr = rcp_nr(pr[0]);
+      cl = sqrt_nr(ph.gamma * pl[4] * rl);
+      cr = sqrt_nr(ph.gamma * pr[4] * rr);
     }
     if constexpr (SOLVER == WX_SOLVER_HLLC) riemann_hllc_c<NEQ>(pl, pr, cl, cr, rl, rr, fx, ph.cv);
     else riemann_hll_c<NEQ>(pl, pr, cl, cr, fx, ph.cv);
@@ -107,6 +116,55 @@ __device__ __forceinline__ void iface_flux(const double* c0, const double* c1, c
   for (int e = 0; e < NEQ; ++e) f[perm<DIR, MHD>(e)] = fx[e];
 }
 
+// Loads plane kk of the slab into its ring slot as primitives: the 16x16
+// physical cells, plus -- for the planes that get x/y fluxes -- the x/y ghost
+// frame (two deep for the second-order stage), gathered from the neighbours.
+template <int NEQ, bool MHD, int ORDER, int CH>
+__device__ __forceinline__ void load_plane(const StageParams& P, const DevBlock& B, int slot, int kk, int z0, int z1,
+                                           double* ring, unsigned& pf, unsigned& df, unsigned& zd) {
+  const int t = threadIdx.x;
+  const PhysParams& ph = P.ph;
+  double* pl = ring + ring_slot(kk) * CH * HPLANE;
+  const bool inner = (kk >= 1 && kk <= NC);
+  const bool frame = (kk >= z0 && kk <= z1);  // plane gets x/y fluxes
+  const int nframe = frame ? (ORDER == 2 ? 128 : 64) : 0;
+  for (int c = t; c < PLANE + nframe; c += STAGE_THREADS) {
+    int i, j;
+    if (c < PLANE) { i = (c & 15) + 1; j = (c >> 4) + 1; }
+    else {
+      const int h = c - PLANE;
+      const int per = ORDER == 2 ? 32 : 16;         // cells per side
+      const int side = h / per, r = (h % 16) + 1;
+      const int d = (ORDER == 2) ? ((h % 32) >> 4) : 1;   // 0: outer, 1: inner ghost layer
+      if (side == 0) { i = d - 1; j = r; }
+      else if (side == 1) { i = NC + 2 - d; j = r; }
+      else if (side == 2) { i = r; j = d - 1; }
+      else { i = r; j = NC + 2 - d; }
+    }
+    double u[NEQ], p[NEQ], rinv;
+    if (inner) get_cell<NEQ>(P.src, B, slot, i, j, kk, u);
+    else gather_ghost<NEQ>(P.src, B, slot, i, j, kk, u);
+    const int st = flow2prim<NEQ, MHD>(u, p, ph.cv, &rinv);
+    if constexpr (CH > NEQ) {
+      pl[NEQ * HPLANE + hidx(i, j)] = sqrt_nr(ph.gamma * p[4] * rinv);
+      pl[(NEQ + 1) * HPLANE + hidx(i, j)] = rinv;
+    }
+    if (c < PLANE && inner && frame) {
+      pf += (st == 1);
+      df += (st == 2);
+      zd += (st < 0);
+    }
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) pl[e * HPLANE + hidx(i, j)] = p[e];
+  }
+}
+
+// Per slab the planes are walked with two barriers each.  Phase A of update
+// plane m loads plane m+ORDER+1 into the slot of plane m-1 (no longer read:
+// the z-interface slope of plane m is carried in registers) while the same
+// threads compute the z-flux m+1/2 and the x/y fluxes of plane m; phase B
+// applies the update.  The loads of one warp overlap the flux arithmetic of
+// the others.
 template <int NEQ, bool MHD, int SOLVER, int ORDER, int LIM>
 __global__ void __launch_bounds__(STAGE_THREADS, (!MHD && NEQ == 5) ? 2 : 1) stage_kernel(StageParams P) {
   constexpr int CH = ring_channels<NEQ, MHD, ORDER>();
@@ -129,61 +187,41 @@ __global__ void __launch_bounds__(STAGE_THREADS, (!MHD && NEQ == 5) ? 2 : 1) sta
     __syncthreads();
     const double dtdx = dtp / B.dx, dtdy = dtp / B.dy, dtdz = dtp / B.dz;
     const int ci = (t & (NC - 1)) + 1, cj = (t >> 4) + 1;   // column of threads t < 256
-    double zprev[NEQ], znew[NEQ];
+    const int hc = hidx(ci, cj);
+    double zprev[NEQ], znew[NEQ], zslope[NEQ];
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e) { zprev[e] = 0.0; znew[e] = 0.0; }
+    for (int e = 0; e < NEQ; ++e) { zprev[e] = 0.0; znew[e] = 0.0; zslope[e] = 0.0; }
+    double bz_below = 0.0;  // B_z of plane m-1 in this thread's column (Powell source)
 
-    for (int kk = z0 - ORDER; kk <= z1 + ORDER; ++kk) {
-      // ---- load plane kk into the ring (conserved -> primitive) ----------
-      __syncthreads();
-      {
-        double* pl = ring + ring_slot(kk) * CH * HPLANE;
-        const bool inner = (kk >= 1 && kk <= NC);
-        const bool frame = (kk >= z0 && kk <= z1);  // plane gets x/y fluxes
-        const int nframe = frame ? (ORDER == 2 ? 128 : 64) : 0;
-        for (int c = t; c < PLANE + nframe; c += STAGE_THREADS) {
-          int i, j;
-          if (c < PLANE) { i = (c & 15) + 1; j = (c >> 4) + 1; }
-          else {
-            const int h = c - PLANE;
-            const int per = ORDER == 2 ? 32 : 16;         // cells per side
-            const int side = h / per, r = (h % 16) + 1;
-            const int d = (ORDER == 2) ? ((h % 32) >> 4) : 1;   // 0: outer, 1: inner ghost layer
-            if (side == 0) { i = d - 1; j = r; }
-            else if (side == 1) { i = NC + 2 - d; j = r; }
-            else if (side == 2) { i = r; j = d - 1; }
-            else { i = r; j = NC + 2 - d; }
-          }
-          double u[NEQ], p[NEQ], rinv;
-          if (inner) get_cell<NEQ>(P.src, B, slot, i, j, kk, u);
-          else gather_ghost<NEQ>(P.src, B, slot, i, j, kk, u);
-          const int st = flow2prim<NEQ, MHD>(u, p, ph.cv, &rinv);
-          if constexpr (CH > NEQ) {
-            pl[NEQ * HPLANE + hidx(i, j)] = sqrt(ph.gamma * p[4] * rinv);
-            pl[(NEQ + 1) * HPLANE + hidx(i, j)] = rinv;
-          }
-          if (c < PLANE && inner && frame) {
-            pf += (st == 1);
-            df += (st == 2);
-            zd += (st < 0);
-          }
+    // ---- prologue: planes z0-ORDER .. z0+ORDER-1, the z-interface z0-1/2,
+    // then plane z0+ORDER into the slot of plane z0-ORDER ------------------
+    for (int kk = z0 - ORDER; kk <= z0 + ORDER - 1; ++kk) load_plane<NEQ, MHD, ORDER, CH>(P, B, slot, kk, z0, z1, ring, pf, df, zd);
+    __syncthreads();
+    if (t < PLANE) {
+      const int m = z0 - 1;
+      const double* c0 = ring + ring_slot(m - 1) * CH * HPLANE + hc;
+      const double* c1 = ring + ring_slot(m) * CH * HPLANE + hc;
+      const double* c2 = ring + ring_slot(m + 1) * CH * HPLANE + hc;
+      const double* c3 = ring + ring_slot(m + 2) * CH * HPLANE + hc;
+      iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 2, true>(c0, c1, c2, c3, ph, znew, zslope, true);
+      if (MHD) bz_below = c1[7 * HPLANE];
+    }
 #pragma unroll
-          for (int e = 0; e < NEQ; ++e) pl[e * HPLANE + hidx(i, j)] = p[e];
-        }
+    for (int e = 0; e < NEQ; ++e) zprev[e] = znew[e];
+    __syncthreads();
+    load_plane<NEQ, MHD, ORDER, CH>(P, B, slot, z0 + ORDER, z0, z1, ring, pf, df, zd);
+    __syncthreads();
+
+    for (int m = z0; m <= z1; ++m) {
+      // ---- phase A: load plane m+ORDER+1; z-flux m+1/2; x/y fluxes of m ---
+      if (m + ORDER + 1 <= z1 + ORDER) load_plane<NEQ, MHD, ORDER, CH>(P, B, slot, m + ORDER + 1, z0, z1, ring, pf, df, zd);
+      if (t < PLANE) {
+        const double* c1 = ring + ring_slot(m) * CH * HPLANE + hc;
+        const double* c2 = ring + ring_slot(m + 1) * CH * HPLANE + hc;
+        const double* c3 = ring + ring_slot(m + 2) * CH * HPLANE + hc;
+        iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 2, true>(nullptr, c1, c2, c3, ph, znew, zslope, false);
       }
-      __syncthreads();
-      const int m = kk - ORDER;  // z-interface m+1/2 and update plane p = m
-      // ---- z-interface m+1/2 of column t ---------------------------------
-      if (m >= z0 - 1 && t < PLANE) {
-        const int h = hidx(ci, cj);
-        const double* c0 = ring + ring_slot(m - 1) * CH * HPLANE + h;
-        const double* c1 = ring + ring_slot(m) * CH * HPLANE + h;
-        const double* c2 = ring + ring_slot(m + 1) * CH * HPLANE + h;
-        const double* c3 = ring + ring_slot(m + 2) * CH * HPLANE + h;
-        iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 2>(c0, c1, c2, c3, ph, znew);
-      }
-      const bool upd = (m >= z0 && m <= z1);
-      if (upd && t < 17 * NC) {
+      if (t < 17 * NC) {
         const double* pp = ring + ring_slot(m) * CH * HPLANE;
         {  // x-interface between ii and ii+1 in row jx
           const int ii = t % 17, jx = t / 17 + 1;
@@ -203,19 +241,18 @@ __global__ void __launch_bounds__(STAGE_THREADS, (!MHD && NEQ == 5) ? 2 : 1) sta
         }
       }
       __syncthreads();
-      // ---- conservative update of plane m (godunov.f90:259-271) ----------
-      if (upd && t < PLANE) {
+      // ---- phase B: conservative update of plane m (godunov.f90:259-271) --
+      if (t < PLANE) {
         double s[NEQ];
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) s[e] = 0.0;
         if (MHD && ph.eight_wave) {  // Powell source (sources.f90:38-95) on the stage primitives
           const double* pm = ring + ring_slot(m) * CH * HPLANE;
-          const double* pd = ring + ring_slot(m - 1) * CH * HPLANE;
           const double* pu = ring + ring_slot(m + 1) * CH * HPLANE;
-          const int h = hidx(ci, cj);
+          const int h = hc;
           const double divB = (pm[5 * HPLANE + h + 1] - pm[5 * HPLANE + h - 1]) / (2. * B.dx) +
                               (pm[6 * HPLANE + h + HW] - pm[6 * HPLANE + h - HW]) / (2. * B.dy) +
-                              (pu[7 * HPLANE + h] - pd[7 * HPLANE + h]) / (2. * B.dz);
+                              (pu[7 * HPLANE + h] - bz_below) / (2. * B.dz);
           const double v1 = pm[1 * HPLANE + h], v2 = pm[2 * HPLANE + h], v3 = pm[3 * HPLANE + h];
           const double b1 = pm[5 * HPLANE + h], b2 = pm[6 * HPLANE + h], b3 = pm[7 * HPLANE + h];
           s[1] = -divB * b1;
@@ -226,6 +263,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, (!MHD && NEQ == 5) ? 2 : 1) sta
           s[6] = -divB * v2;
           s[7] = -divB * v3;
         }
+        if (MHD) bz_below = ring[ring_slot(m) * CH * HPLANE + 7 * HPLANE + hc];
         const size_t o = cell_off(slot, NEQ, 0, ci, cj, m);
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) {
@@ -239,6 +277,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, (!MHD && NEQ == 5) ? 2 : 1) sta
       }
 #pragma unroll
       for (int e = 0; e < NEQ; ++e) zprev[e] = znew[e];
+      __syncthreads();
     }
   }
   flush_counts(P.ctl, pf, df, zd);
