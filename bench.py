@@ -330,7 +330,8 @@ def main():
                        "l2": "state arrays larger than L2 (%.2f GB each)" % (state_bytes / 1e9),
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "path": "wx3d_run: CUDA graph of 2 steps replayed",
-                       "autotune": tuned and {"zsplit": tuned["zsplit"], "ms_per_pass": tuned["ms_per_pass"]}},
+                       "autotune": tuned and {"zsplit": tuned["zsplit"], "fused_viscous": tuned.get("fused"),
+                                              "ms_per_pass": tuned["ms_per_pass"]}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "kernel": "stage_kernel<ORDER=2> (corrector)", "peak_source": peak_src,

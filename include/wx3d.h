@@ -170,12 +170,20 @@ int wx3d_get_neighbours(wx_ctx* ctx, int32_t nslots, int32_t* face_type, int32_t
  * wx3d_set_mesh picks a default; the autotuner overrides it. */
 int wx3d_set_zsplit(wx_ctx* ctx, int32_t zsplit);
 
+/* With fusion on (the default) and whole blocks per CTA (zsplit 1), the
+ * corrector stage also applies doViscousStep; otherwise a separate viscous
+ * kernel runs after it.  The autotuner overrides the choice. */
+int wx3d_set_fusion(wx_ctx* ctx, int32_t fuse_viscous);
+
 /* Autotuner of the stage launch shape for the current mesh: times the
- * predictor and corrector stages (reps passes each) for z-slab splits
- * 1, 2, 4, 8 -- on the live state, without changing it -- and keeps the
- * fastest.  ms4 (may be NULL) receives the time per pass of each split,
- * *best (may be NULL) the chosen split. */
-int wx3d_autotune(wx_ctx* ctx, int32_t reps, double* ms4, int32_t* best);
+ * predictor, the corrector and the viscous step (reps passes each) -- on
+ * the live state, without changing it -- for five shapes: whole blocks with
+ * the viscous step fused into the corrector, whole blocks with a separate
+ * viscous kernel, and 2, 4, 8 z-slabs per block; keeps the fastest.
+ * ms5 (may be NULL) receives the time per pass of each shape in that
+ * order, best (may be NULL) two values: the chosen split and the fusion
+ * flag. */
+int wx3d_autotune(wx_ctx* ctx, int32_t reps, double* ms5, int32_t* best);
 
 /* Conserved variables, native layout: u[slot][eq][k][j][i], 16^3 physical
  * cells per block, host memory (pinned or pageable). */

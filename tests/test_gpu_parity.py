@@ -366,3 +366,55 @@ def test_fast_reciprocal_and_sqrt_within_two_ulp():
                                   out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
     assert rc == 0
     assert out[0] <= 2 and out[1] <= 2, out
+
+
+def _shape(g, shape):
+    g.set_zsplit(int(shape.split("-")[0]))
+    g.set_fusion(shape.endswith("fused"))
+
+
+@pytest.mark.parametrize("shape", ["1-fused", "1", "2", "8"])
+def test_launch_shapes_match_oracle(shape, ncpu):
+    """Every launch shape of the stage kernels (whole blocks with the viscous
+    step fused into the corrector or separate, 2 and 8 z-slabs) against the
+    CPU oracle on the three-level AMR mesh."""
+    prob = small_amr()
+    o = oracle.from_problem(prob, threads=ncpu)
+    g = from_problem(prob)
+    _shape(g, shape)
+    for _ in range(10):
+        o.step()
+        g.step()
+    check(o, g, prob)
+
+
+@pytest.mark.parametrize("name", ["amr", "brio-wu", "snr-h"])
+def test_fused_viscous_step_equals_separate_kernel(name, ncpu):
+    """The corrector with the viscous step fused reproduces the separate
+    viscous kernel: hydro AMR (CFL from the viscous result), MHD with the
+    8-wave source, and the radiative SNR (CFL from the source step)."""
+    prob = {"amr": small_amr, "brio-wu": lambda: problems.brio_wu(4),
+            "snr-h": lambda: problems.snr_h(nroot=2, maxlev=2)}[name]()
+    a, b = from_problem(prob), from_problem(prob)
+    _shape(a, "1-fused")
+    _shape(b, "1")
+    sa, sb = a.run(8), b.run(8)
+    Ua, Ub = a.download(), b.download()
+    assert np.all(np.isfinite(Ua))
+    assert rel_l1(Ua, Ub).max() <= 1e-14
+    assert sa.dt == pytest.approx(sb.dt, rel=1e-14) and sa.it == sb.it
+    if name == "brio-wu":
+        o = oracle.from_problem(prob, threads=ncpu)
+        for _ in range(8):
+            o.step()
+        check(o, a, prob)
+
+
+def test_autotune_picks_a_shape_and_keeps_the_state():
+    prob = small_amr()
+    g = from_problem(prob)
+    U0 = g.download()
+    z, fused, ms = g.autotune(2)
+    assert z in (1, 2, 4, 8) and set(ms) == set(g.SHAPES) and all(v > 0 for v in ms.values())
+    assert fused in (True, False)
+    assert np.array_equal(g.download(), U0)

@@ -2,10 +2,12 @@
 
 The stage kernels run one CTA per (block, z-slab).  How many slabs a block
 is cut into trades parallelism (small meshes leave SMs idle) against
-redundant halo planes (each slab reloads two planes on either side).  The
-best split depends on the block count, the levels and the equation set, so
-it is measured on the live mesh (wx3d_autotune) and cached by a workload
-signature in a JSON file.
+redundant halo planes (each slab reloads two planes on either side).  With
+whole blocks the corrector can also carry the viscous step, which saves a
+pass over the state but needs more shared memory per CTA (fewer CTAs per
+SM for the passive-scalar equation sets).  The best shape depends on the
+block count, the levels and the equation set, so it is measured on the live
+mesh (wx3d_autotune) and cached by a workload signature in a JSON file.
 """
 from __future__ import annotations
 
@@ -22,7 +24,7 @@ def signature(cfg, nblocks: int, levels) -> str:
 
 
 def tune(w, prob, cache: Path | None = DEFAULT_CACHE, reps: int = 3, force: bool = False) -> dict:
-    """Picks the z-slab split for w's mesh; returns a record of the choice."""
+    """Picks the launch shape for w's mesh; returns a record of the choice."""
     levels = [prob.tree.level(int(b)) for b in prob.local_blocks]
     key = signature(prob.cfg, prob.nblocks, levels)
     table = {}
@@ -31,11 +33,12 @@ def tune(w, prob, cache: Path | None = DEFAULT_CACHE, reps: int = 3, force: bool
             table = json.loads(cache.read_text())
         except ValueError:
             table = {}
-    if key in table and not force:
+    if key in table and not force and "fused" in table[key]:
         w.set_zsplit(int(table[key]["zsplit"]))
+        w.set_fusion(bool(table[key]["fused"]))
         return dict(table[key], cached=True, key=key)
-    best, ms = w.autotune(reps)
-    rec = {"zsplit": best, "ms_per_pass": {str(k): v for k, v in ms.items()}}
+    best, fused, ms = w.autotune(reps)
+    rec = {"zsplit": best, "fused": fused, "ms_per_pass": {str(k): v for k, v in ms.items()}}
     if cache is not None:
         cache.parent.mkdir(parents=True, exist_ok=True)
         table[key] = rec

@@ -30,6 +30,7 @@ namespace {
 struct Kern {
   void (*stage1)(StageParams) = nullptr;
   void (*stage2)(StageParams) = nullptr;
+  void (*stage2v)(StageParams) = nullptr;  // corrector with the viscous step fused
   void (*lax)(LaxParams) = nullptr;
   void (*visc)(ViscParams) = nullptr;
   void (*dt)(DtParams) = nullptr;
@@ -38,6 +39,7 @@ struct Kern {
   void (*prims)(const double*, double*, const int32_t*, int, DevCtl*, double) = nullptr;
   size_t smem1 = 0;  // dynamic shared memory of the predictor and the corrector
   size_t smem2 = 0;
+  size_t smem2v = 0;
 };
 
 template <int NEQ, bool MHD, int SOLVER, int LIM>
@@ -45,6 +47,7 @@ Kern make_kern() {
   Kern k;
   k.stage1 = stage_kernel<NEQ, MHD, SOLVER, 1, LIM_RUNTIME>;
   k.stage2 = stage_kernel<NEQ, MHD, SOLVER, 2, LIM>;
+  k.stage2v = stage_kernel<NEQ, MHD, SOLVER, 2, LIM, true>;
   k.lax = lax_kernel<NEQ, MHD>;
   k.visc = viscous_kernel<NEQ, MHD>;
   k.dt = dt_kernel<NEQ, MHD>;
@@ -53,6 +56,7 @@ Kern make_kern() {
   k.prims = prims_kernel<NEQ, MHD>;
   k.smem1 = stage_smem_bytes<NEQ, MHD, 1>();
   k.smem2 = stage_smem_bytes<NEQ, MHD, 2>();
+  k.smem2v = stage_smem_bytes<NEQ, MHD, 2, true>();
   return k;
 }
 
@@ -161,6 +165,7 @@ struct wx_ctx {
   std::vector<DevBlock> hblocks;
   int nwork = 0;
   int zsplit = 1;
+  bool fuse = true;   // corrector carries the viscous step when zsplit == 1
   int grid_stage = 0, grid_256 = 0;
   bool dt_valid = false;
   bool prestep = false;           // dW holds the state at the start of the last step
@@ -274,6 +279,7 @@ int grid_for(wx_ctx* c, const void* fn, int threads, size_t smem, int items) {
 int set_stage_attrs(wx_ctx* c) {
   WX_CUDA(cudaFuncSetAttribute(c->k.stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->k.smem1));
   WX_CUDA(cudaFuncSetAttribute(c->k.stage2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->k.smem2));
+  WX_CUDA(cudaFuncSetAttribute(c->k.stage2v, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->k.smem2v));
   return WX_OK;
 }
 
@@ -288,10 +294,13 @@ int launch_dt(wx_ctx* c, const double* u) {
   return WX_OK;
 }
 
-int launch_stage(wx_ctx* c, int order, const double* src, const double* base, double* out, double factor) {
-  StageParams P{src, base, out, c->dBlocks, c->dWork, c->nwork * c->zsplit, c->zsplit, c->dCtl, factor, c->ph};
-  auto fn = order == 1 ? c->k.stage1 : c->k.stage2;
-  const size_t smem = order == 1 ? c->k.smem1 : c->k.smem2;
+// fused: the corrector that also applies doViscousStep (whole blocks only)
+int launch_stage(wx_ctx* c, int order, const double* src, const double* base, double* out, double factor,
+                 bool fused = false) {
+  StageParams P{src, base, out, c->dBlocks, c->dWork, c->nwork * c->zsplit, c->zsplit, c->dCtl, factor, c->ph,
+                sources_on(c) ? 0 : 1};
+  auto fn = order == 1 ? c->k.stage1 : (fused ? c->k.stage2v : c->k.stage2);
+  const size_t smem = order == 1 ? c->k.smem1 : (fused ? c->k.smem2v : c->k.smem2);
   const int grid = grid_for(c, (const void*)fn, STAGE_THREADS, smem, c->nwork * c->zsplit);
   const int kind = (order == 2 || factor == 1.0) ? 1 : 0;
   tick(c, kind, true);
@@ -299,6 +308,22 @@ int launch_stage(wx_ctx* c, int order, const double* src, const double* base, do
   WX_LAUNCHED();
   tick(c, kind, false);
   return WX_OK;
+}
+
+// doViscousStep on dW in place, UP ghosts (zero for single-stage solvers)
+int launch_visc(wx_ctx* c, int zero_ghost) {
+  ViscParams V{c->dW, c->dUP, c->dBlocks, c->dWork, c->nwork, zero_ghost, sources_on(c) ? 0 : 1, c->dCtl, c->ph};
+  tick(c, 2, true);
+  c->k.visc<<<grid_for(c, (const void*)c->k.visc, 256, 0, c->nwork), 256, 0, c->stream>>>(V);
+  WX_LAUNCHED();
+  tick(c, 2, false);
+  return WX_OK;
+}
+
+// The corrector carries the viscous step when every block is one slab.
+bool fuse_visc(const wx_ctx* c) {
+  const int s = c->cfg.solver_type;
+  return c->fuse && c->zsplit == 1 && s != WX_SOLVER_LAX && s != WX_SOLVER_HLL1;
 }
 
 // Godunov(order)/LaxFriedrichs + doViscousStep; on return dU holds U^{n+1}.
@@ -322,13 +347,9 @@ int enqueue_solver(wx_ctx* c, bool bump_it, bool finish_output) {
     zero_ghost = 1;
   } else {
     if ((rc = launch_stage(c, 1, c->dU, c->dU, c->dUP, 0.5))) return rc;
-    if ((rc = launch_stage(c, 2, c->dUP, c->dU, c->dW, 1.0))) return rc;
+    if ((rc = launch_stage(c, 2, c->dUP, c->dU, c->dW, 1.0, fuse_visc(c)))) return rc;
   }
-  ViscParams V{c->dW, c->dUP, c->dBlocks, c->dWork, c->nwork, zero_ghost, src ? 0 : 1, c->dCtl, c->ph};
-  tick(c, 2, true);
-  c->k.visc<<<grid_for(c, (const void*)c->k.visc, 256, 0, c->nwork), 256, 0, c->stream>>>(V);
-  WX_LAUNCHED();
-  tick(c, 2, false);
+  if (!fuse_visc(c) && (rc = launch_visc(c, zero_ghost))) return rc;
   step_end_kernel<<<1, 1, 0, c->stream>>>(c->dCtl, finish_output ? 1 : 0);
   WX_LAUNCHED();
   std::swap(c->dU, c->dW);
@@ -632,10 +653,17 @@ int wx3d_set_zsplit(wx_ctx* c, int32_t zsplit) {
 // Measured choice of the z-slab split: times the predictor and corrector
 // stages (which write only the UP and W scratch arrays, so U and the
 // simulation state are untouched) for every split and keeps the fastest.
-int wx3d_autotune(wx_ctx* c, int32_t reps, double* ms4, int32_t* best) {
+int wx3d_set_fusion(wx_ctx* c, int32_t on) {
+  if (!c) return WX_ERR_INVALID_ARG;
+  c->fuse = on != 0;
+  invalidate_graph(c);
+  return WX_OK;
+}
+
+int wx3d_autotune(wx_ctx* c, int32_t reps, double* ms5, int32_t* best) {
   if (!ready(c) || reps <= 0) return WX_ERR_INVALID_ARG;
   if (c->cfg.solver_type == WX_SOLVER_LAX) {
-    if (best) *best = 1;
+    if (best) { best[0] = 1; best[1] = 0; }
     return WX_OK;
   }
   int rc;
@@ -648,33 +676,41 @@ int wx3d_autotune(wx_ctx* c, int32_t reps, double* ms4, int32_t* best) {
   WX_CUDA(cudaEventCreate(&e1));
   const bool timing = c->timing;
   c->timing = false;
-  const int splits[4] = {1, 2, 4, 8};
+  // launch shapes: whole blocks with the fused corrector, whole blocks with
+  // a separate viscous kernel, then 2, 4 and 8 slabs per block
+  const int splits[5] = {1, 1, 2, 4, 8};
+  const bool fused[5] = {true, false, false, false, false};
   double bestms = 1e300;
   int bz = c->zsplit;
-  for (int s = 0; s < 4; ++s) {
+  bool bf = c->fuse;
+  const bool hll1 = c->cfg.solver_type == WX_SOLVER_HLL1;
+  for (int s = 0; s < 5; ++s) {
     c->zsplit = splits[s];
-    // one untimed pass, then reps timed passes of both stages
+    c->fuse = fused[s];
+    // one untimed pass, then reps timed passes of both stages and the
+    // viscous step
     for (int r = 0; r <= reps; ++r) {
       if (r == 1) cudaEventRecord(e0, c->stream);
-      if ((rc = launch_stage(c, 1, c->dU, c->dU, c->dUP, 0.5))) { c->timing = timing; return rc; }
-      if (c->cfg.solver_type != WX_SOLVER_HLL1 && (rc = launch_stage(c, 2, c->dUP, c->dU, c->dW, 1.0))) {
-        c->timing = timing;
-        return rc;
-      }
+      if ((rc = launch_stage(c, 1, c->dU, c->dU, hll1 ? c->dW : c->dUP, hll1 ? 1.0 : 0.5))) break;
+      if (!hll1 && (rc = launch_stage(c, 2, c->dUP, c->dU, c->dW, 1.0, fuse_visc(c)))) break;
+      if (!fuse_visc(c) && (rc = launch_visc(c, hll1 ? 1 : 0))) break;
     }
+    if (rc) break;
     cudaEventRecord(e1, c->stream);
     WX_CUDA(cudaEventSynchronize(e1));
     float ms = 0.f;
     WX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     const double per = ms / reps;
-    if (ms4) ms4[s] = per;
-    if (per < bestms) { bestms = per; bz = splits[s]; }
+    if (ms5) ms5[s] = per;
+    if (per < bestms) { bestms = per; bz = splits[s]; bf = fused[s]; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   c->timing = timing;
   c->zsplit = bz;
-  if (best) *best = bz;
+  c->fuse = bf;
+  if (rc) return rc;
+  if (best) { best[0] = bz; best[1] = bf ? 1 : 0; }
   invalidate_graph(c);
   return WX_OK;
 }
@@ -1289,6 +1325,7 @@ extern "C" int wx3d_hydro_step_noalloc(const wx_config* cfg, int32_t nslots, con
   }
   if (nwork == 0) return WX_ERR_MESH;
   int zsplit = 1;
+  bool fuse = true;   // corrector carries the viscous step when zsplit == 1
   while (zsplit < 8 && nwork * zsplit < 2 * nsm) zsplit *= 2;
 
   PhysParams ph{};

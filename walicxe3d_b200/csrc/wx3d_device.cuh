@@ -19,8 +19,6 @@ namespace wx {
 constexpr int NC = WX3D_NCELLS;
 constexpr int PLANE = NC * NC;          // 256 cells per k-plane
 constexpr int BCELLS = NC * NC * NC;    // 4096 cells per block
-constexpr int HW = NC + 4;              // 20: plane width with two ghost layers each side
-constexpr int HPLANE = HW * HW;         // 400
 
 // One slot of the device neighbour table (built on the host from the
 // reference's tree queries, source/amr.f90:439-1098).

@@ -26,6 +26,14 @@ struct StageParams {
   DevCtl* ctl;
   double dt_factor;                 // 0.5 for the predictor, 1 otherwise
   PhysParams ph;
+  int32_t do_dt;                    // fused viscous step: fold the CFL minimum of the result
+};
+
+// Ring plane geometry: 16x16 cells with the ORDER-deep x/y ghost frame.
+template <int ORDER>
+struct Geo {
+  static constexpr int W = NC + 2 * ORDER;   // 20 for the corrector, 18 for the predictor
+  static constexpr int PL = W * W;
 };
 
 // Ring channels per cell: the primitives, plus -- for the first-order hydro
@@ -37,14 +45,28 @@ __host__ __device__ constexpr int ring_channels() {
   return NEQ + ((!MHD && ORDER == 1) ? 2 : 0);
 }
 
-template <int NEQ, bool MHD, int ORDER>
+constexpr int VPLANE = (NC + 2) * (NC + 2);  // a plane with its one-deep x/y frame
+
+template <int NEQ, bool MHD, int ORDER, bool VISC = false>
 __host__ __device__ constexpr size_t stage_smem_bytes() {
-  return sizeof(double) * ((size_t)RING * ring_channels<NEQ, MHD, ORDER>() * HPLANE + 2 * (size_t)NEQ * 17 * NC) +
+  return sizeof(double) * ((size_t)RING * ring_channels<NEQ, MHD, ORDER>() * Geo<ORDER>::PL + 2 * (size_t)NEQ * 17 * NC +
+                           (VISC ? 2 * (size_t)NEQ * VPLANE : 0)) +
          sizeof(DevBlock);
 }
 
-__device__ __forceinline__ int hidx(int i, int j) { return (i + 1) + HW * (j + 1); }
+template <int ORDER>
+__device__ __forceinline__ int hidx(int i, int j) { return (i + ORDER - 1) + Geo<ORDER>::W * (j + ORDER - 1); }
 __device__ __forceinline__ int ring_slot(int kk) { return (kk + 64) & (RING - 1); }
+
+// Warp minimum of a positive time step folded into ctl->dtmin_bits.
+__device__ __forceinline__ void block_min_dt(double v, DevCtl* ctl) {
+  v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 16));
+  v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 8));
+  v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 4));
+  v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 2));
+  v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 1));
+  if ((threadIdx.x & 31) == 0) atomic_min_pos(&ctl->dtmin_bits, v);
+}
 
 // Block-wide sum of four status counters into ctl->cnt.
 __device__ __forceinline__ void flush_counts(DevCtl* ctl, unsigned pf, unsigned df, unsigned zd) {
@@ -60,7 +82,7 @@ __device__ __forceinline__ void flush_counts(DevCtl* ctl, unsigned pf, unsigned 
 }
 
 // One interface flux in direction DIR from ring cells c0..c3 (pointers to
-// equation 0 of cells l-1, l, r, r+1; stride HPLANE between channels).
+// equation 0 of cells l-1, l, r, r+1; stride Geo<ORDER>::PL between channels).
 // With CARRY (the z-interfaces, which a thread visits in order along its
 // column) the limited slope of the lower cell is the upper cell's slope of
 // the previous interface -- the limiter sees the same two differences -- and
@@ -74,17 +96,17 @@ __device__ __forceinline__ void iface_flux(const double* c0, const double* c1, c
 #pragma unroll
   for (int e = 0; e < NEQ; ++e) {
     const int q = perm<DIR, MHD>(e);
-    pl[e] = c1[q * HPLANE];
-    pr[e] = c2[q * HPLANE];
+    pl[e] = c1[q * Geo<ORDER>::PL];
+    pr[e] = c2[q * Geo<ORDER>::PL];
   }
   if (ORDER == 2) {  // limiter (hydro_core.f90:613-636) on permuted primitives
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) {
       const int q = perm<DIR, MHD>(e);
-      const double prr = c3[q * HPLANE];
+      const double prr = c3[q * Geo<ORDER>::PL];
       const double dm = pr[e] - pl[e], dr = prr - pr[e];
       double al;
-      if (!CARRY || first) al = average_t<LIM>(pl[e] - c0[q * HPLANE], dm, ph.limiter);
+      if (!CARRY || first) al = average_t<LIM>(pl[e] - c0[q * Geo<ORDER>::PL], dm, ph.limiter);
       else al = carry[e];
       const double ar = average_t<LIM>(dm, dr, ph.limiter);
       if (CARRY) carry[e] = ar;
@@ -95,10 +117,10 @@ __device__ __forceinline__ void iface_flux(const double* c0, const double* c1, c
   if constexpr (!MHD && (SOLVER == WX_SOLVER_HLL || SOLVER == WX_SOLVER_HLLC)) {
     double cl, cr, rl, rr;
     if constexpr (ORDER == 1) {  // cell values: sound speed and 1/rho from the ring
-      cl = c1[NEQ * HPLANE];
-      cr = c2[NEQ * HPLANE];
-      rl = c1[(NEQ + 1) * HPLANE];
-      rr = c2[(NEQ + 1) * HPLANE];
+      cl = c1[NEQ * Geo<ORDER>::PL];
+      cr = c2[NEQ * Geo<ORDER>::PL];
+      rl = c1[(NEQ + 1) * Geo<ORDER>::PL];
+      rr = c2[(NEQ + 1) * Geo<ORDER>::PL];
     } else {
       rl = rcp_nr(pl[0]);
       rr = rcp_nr(pr[0]);
@@ -116,6 +138,23 @@ __device__ __forceinline__ void iface_flux(const double* c0, const double* c1, c
   for (int e = 0; e < NEQ; ++e) f[perm<DIR, MHD>(e)] = fx[e];
 }
 
+// Stores the result of the fused viscous step for one cell, counts
+// non-finite values and folds the cell's CFL time step.
+template <int NEQ, bool MHD>
+__device__ __forceinline__ void visc_store(const StageParams& P, const DevBlock& B, const double* un, size_t o,
+                                           double& dtl, unsigned& nonfinite) {
+#pragma unroll
+  for (int e = 0; e < NEQ; ++e) {
+    P.out[o + (size_t)e * BCELLS] = un[e];
+    nonfinite += !isfinite(un[e]);
+  }
+  if (P.do_dt) {
+    double p[NEQ];
+    flow2prim<NEQ, MHD>(un, p, P.ph.cv);
+    dtl = dmin(dtl, cell_dt<NEQ, MHD>(p, B, P.ph.gamma));
+  }
+}
+
 // Loads plane kk of the slab into its ring slot as primitives: the 16x16
 // physical cells, plus -- for the planes that get x/y fluxes -- the x/y ghost
 // frame (two deep for the second-order stage), gathered from the neighbours.
@@ -124,7 +163,7 @@ __device__ __forceinline__ void load_plane(const StageParams& P, const DevBlock&
                                            double* ring, unsigned& pf, unsigned& df, unsigned& zd) {
   const int t = threadIdx.x;
   const PhysParams& ph = P.ph;
-  double* pl = ring + ring_slot(kk) * CH * HPLANE;
+  double* pl = ring + ring_slot(kk) * CH * Geo<ORDER>::PL;
   const bool inner = (kk >= 1 && kk <= NC);
   const bool frame = (kk >= z0 && kk <= z1);  // plane gets x/y fluxes
   const int nframe = frame ? (ORDER == 2 ? 128 : 64) : 0;
@@ -146,8 +185,8 @@ __device__ __forceinline__ void load_plane(const StageParams& P, const DevBlock&
     else gather_ghost<NEQ>(P.src, B, slot, i, j, kk, u);
     const int st = flow2prim<NEQ, MHD>(u, p, ph.cv, &rinv);
     if constexpr (CH > NEQ) {
-      pl[NEQ * HPLANE + hidx(i, j)] = sqrt_nr(ph.gamma * p[4] * rinv);
-      pl[(NEQ + 1) * HPLANE + hidx(i, j)] = rinv;
+      pl[NEQ * Geo<ORDER>::PL + hidx<ORDER>(i, j)] = sqrt_nr(ph.gamma * p[4] * rinv);
+      pl[(NEQ + 1) * Geo<ORDER>::PL + hidx<ORDER>(i, j)] = rinv;
     }
     if (c < PLANE && inner && frame) {
       pf += (st == 1);
@@ -155,7 +194,7 @@ __device__ __forceinline__ void load_plane(const StageParams& P, const DevBlock&
       zd += (st < 0);
     }
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e) pl[e * HPLANE + hidx(i, j)] = p[e];
+    for (int e = 0; e < NEQ; ++e) pl[e * Geo<ORDER>::PL + hidx<ORDER>(i, j)] = p[e];
   }
 }
 
@@ -165,14 +204,33 @@ __device__ __forceinline__ void load_plane(const StageParams& P, const DevBlock&
 // threads compute the z-flux m+1/2 and the x/y fluxes of plane m; phase B
 // applies the update.  The loads of one warp overlap the flux arithmetic of
 // the others.
-template <int NEQ, bool MHD, int SOLVER, int ORDER, int LIM>
-__global__ void __launch_bounds__(STAGE_THREADS, (!MHD && NEQ == 5) ? 2 : 1) stage_kernel(StageParams P) {
+//
+// VISC (second stage, whole blocks) fuses doViscousStep
+// (hydro_solver.f90:217-250): the stage result W of plane m goes to a
+// two-plane shared buffer whose one-deep x/y frame holds the half-step UP
+// ghosts, and phase B of plane m applies U = W + eta (sum of the six
+// neighbours - 6 W) to plane m-1, whose z-neighbours are W(m-2) (still in
+// the buffer slot that W(m) replaces, read first by the same thread) and
+// W(m) (in registers).  The block-face z-neighbours are UP ghosts as well.
+// Two CTAs per SM where the shared memory allows it; registers are then
+// capped at 96 per thread (nine warps per CTA, five on one sub-partition).
+template <int NEQ, bool MHD, int ORDER, bool VISC>
+__host__ __device__ constexpr int stage_ctas_per_sm() {
+  return (!MHD && 2 * (stage_smem_bytes<NEQ, MHD, ORDER, VISC>() + 1024) <= 228 * 1024) ? 2 : 1;
+}
+
+template <int NEQ, bool MHD, int SOLVER, int ORDER, int LIM, bool VISC = false>
+__global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, ORDER, VISC>())) stage_kernel(StageParams P) {
   constexpr int CH = ring_channels<NEQ, MHD, ORDER>();
   extern __shared__ __align__(16) double smem[];
-  double* ring = smem;                                   // [RING][CH][HPLANE]
-  double* fxs = ring + RING * CH * HPLANE;               // [NEQ][16 rows][17]
+  double* ring = smem;                                   // [RING][CH][Geo<ORDER>::PL]
+  double* fxs = ring + RING * CH * Geo<ORDER>::PL;               // [NEQ][16 rows][17]
   double* fys = fxs + NEQ * 17 * NC;                     // [NEQ][17][16 cols]
-  DevBlock& B = *reinterpret_cast<DevBlock*>(fys + NEQ * 17 * NC);
+  double* wpl = fys + NEQ * 17 * NC;                     // VISC: [2][NEQ][VPLANE]
+  DevBlock& B = *reinterpret_cast<DevBlock*>(wpl + (VISC ? 2 * NEQ * VPLANE : 0));
+  auto vq = [](int i, int j) { return i + (NC + 2) * j; };
+  double dtl = 1.0e300;
+  unsigned nonfinite = 0;
   const int t = threadIdx.x;
   const int planes = NC / P.zsplit;
   const PhysParams& ph = P.ph;
@@ -187,7 +245,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, (!MHD && NEQ == 5) ? 2 : 1) sta
     __syncthreads();
     const double dtdx = dtp / B.dx, dtdy = dtp / B.dy, dtdz = dtp / B.dz;
     const int ci = (t & (NC - 1)) + 1, cj = (t >> 4) + 1;   // column of threads t < 256
-    const int hc = hidx(ci, cj);
+    const int hc = hidx<ORDER>(ci, cj);
     double zprev[NEQ], znew[NEQ], zslope[NEQ];
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) { zprev[e] = 0.0; znew[e] = 0.0; zslope[e] = 0.0; }
@@ -199,15 +257,21 @@ __global__ void __launch_bounds__(STAGE_THREADS, (!MHD && NEQ == 5) ? 2 : 1) sta
     __syncthreads();
     if (t < PLANE) {
       const int m = z0 - 1;
-      const double* c0 = ring + ring_slot(m - 1) * CH * HPLANE + hc;
-      const double* c1 = ring + ring_slot(m) * CH * HPLANE + hc;
-      const double* c2 = ring + ring_slot(m + 1) * CH * HPLANE + hc;
-      const double* c3 = ring + ring_slot(m + 2) * CH * HPLANE + hc;
+      const double* c0 = ring + ring_slot(m - 1) * CH * Geo<ORDER>::PL + hc;
+      const double* c1 = ring + ring_slot(m) * CH * Geo<ORDER>::PL + hc;
+      const double* c2 = ring + ring_slot(m + 1) * CH * Geo<ORDER>::PL + hc;
+      const double* c3 = ring + ring_slot(m + 2) * CH * Geo<ORDER>::PL + hc;
       iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 2, true>(c0, c1, c2, c3, ph, znew, zslope, true);
-      if (MHD) bz_below = c1[7 * HPLANE];
+      if (MHD) bz_below = c1[7 * Geo<ORDER>::PL];
     }
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) zprev[e] = znew[e];
+    if (VISC && t < PLANE) {  // W(z0-1) of the column: the bottom UP ghost
+      double g[NEQ];
+      gather_ghost<NEQ>(P.src, B, slot, ci, cj, z0 - 1, g);
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e) wpl[((z0 - 1) & 1) * NEQ * VPLANE + e * VPLANE + vq(ci, cj)] = g[e];
+    }
     __syncthreads();
     load_plane<NEQ, MHD, ORDER, CH>(P, B, slot, z0 + ORDER, z0, z1, ring, pf, df, zd);
     __syncthreads();
@@ -215,27 +279,38 @@ __global__ void __launch_bounds__(STAGE_THREADS, (!MHD && NEQ == 5) ? 2 : 1) sta
     for (int m = z0; m <= z1; ++m) {
       // ---- phase A: load plane m+ORDER+1; z-flux m+1/2; x/y fluxes of m ---
       if (m + ORDER + 1 <= z1 + ORDER) load_plane<NEQ, MHD, ORDER, CH>(P, B, slot, m + ORDER + 1, z0, z1, ring, pf, df, zd);
+      if (VISC && t >= PLANE) {  // one-deep x/y frame of W(m): UP ghosts of plane m
+        for (int f = t - PLANE; f < 4 * NC; f += STAGE_THREADS - PLANE) {
+          const int side = f >> 4, r = (f & 15) + 1;
+          const int gi = side == 0 ? 0 : (side == 1 ? NC + 1 : r);
+          const int gj = side == 2 ? 0 : (side == 3 ? NC + 1 : r);
+          double g[NEQ];
+          gather_ghost<NEQ>(P.src, B, slot, gi, gj, m, g);
+#pragma unroll
+          for (int e = 0; e < NEQ; ++e) wpl[(m & 1) * NEQ * VPLANE + e * VPLANE + vq(gi, gj)] = g[e];
+        }
+      }
       if (t < PLANE) {
-        const double* c1 = ring + ring_slot(m) * CH * HPLANE + hc;
-        const double* c2 = ring + ring_slot(m + 1) * CH * HPLANE + hc;
-        const double* c3 = ring + ring_slot(m + 2) * CH * HPLANE + hc;
+        const double* c1 = ring + ring_slot(m) * CH * Geo<ORDER>::PL + hc;
+        const double* c2 = ring + ring_slot(m + 1) * CH * Geo<ORDER>::PL + hc;
+        const double* c3 = ring + ring_slot(m + 2) * CH * Geo<ORDER>::PL + hc;
         iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 2, true>(nullptr, c1, c2, c3, ph, znew, zslope, false);
       }
       if (t < 17 * NC) {
-        const double* pp = ring + ring_slot(m) * CH * HPLANE;
+        const double* pp = ring + ring_slot(m) * CH * Geo<ORDER>::PL;
         {  // x-interface between ii and ii+1 in row jx
           const int ii = t % 17, jx = t / 17 + 1;
           double f[NEQ];
-          iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 0>(pp + hidx(ii - 1, jx), pp + hidx(ii, jx), pp + hidx(ii + 1, jx),
-                                                 pp + hidx(ii + 2, jx), ph, f);
+          iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 0>(pp + hidx<ORDER>(ii - 1, jx), pp + hidx<ORDER>(ii, jx), pp + hidx<ORDER>(ii + 1, jx),
+                                                 pp + hidx<ORDER>(ii + 2, jx), ph, f);
 #pragma unroll
           for (int e = 0; e < NEQ; ++e) fxs[(e * NC + (jx - 1)) * 17 + ii] = f[e];
         }
         {  // y-interface between jj and jj+1 in column iy
           const int iy = (t & 15) + 1, jj = t >> 4;
           double f[NEQ];
-          iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 1>(pp + hidx(iy, jj - 1), pp + hidx(iy, jj), pp + hidx(iy, jj + 1),
-                                                 pp + hidx(iy, jj + 2), ph, f);
+          iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 1>(pp + hidx<ORDER>(iy, jj - 1), pp + hidx<ORDER>(iy, jj), pp + hidx<ORDER>(iy, jj + 1),
+                                                 pp + hidx<ORDER>(iy, jj + 2), ph, f);
 #pragma unroll
           for (int e = 0; e < NEQ; ++e) fys[(e * 17 + jj) * NC + (iy - 1)] = f[e];
         }
@@ -247,14 +322,14 @@ __global__ void __launch_bounds__(STAGE_THREADS, (!MHD && NEQ == 5) ? 2 : 1) sta
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) s[e] = 0.0;
         if (MHD && ph.eight_wave) {  // Powell source (sources.f90:38-95) on the stage primitives
-          const double* pm = ring + ring_slot(m) * CH * HPLANE;
-          const double* pu = ring + ring_slot(m + 1) * CH * HPLANE;
+          const double* pm = ring + ring_slot(m) * CH * Geo<ORDER>::PL;
+          const double* pu = ring + ring_slot(m + 1) * CH * Geo<ORDER>::PL;
           const int h = hc;
-          const double divB = (pm[5 * HPLANE + h + 1] - pm[5 * HPLANE + h - 1]) / (2. * B.dx) +
-                              (pm[6 * HPLANE + h + HW] - pm[6 * HPLANE + h - HW]) / (2. * B.dy) +
-                              (pu[7 * HPLANE + h] - bz_below) / (2. * B.dz);
-          const double v1 = pm[1 * HPLANE + h], v2 = pm[2 * HPLANE + h], v3 = pm[3 * HPLANE + h];
-          const double b1 = pm[5 * HPLANE + h], b2 = pm[6 * HPLANE + h], b3 = pm[7 * HPLANE + h];
+          const double divB = (pm[5 * Geo<ORDER>::PL + h + 1] - pm[5 * Geo<ORDER>::PL + h - 1]) / (2. * B.dx) +
+                              (pm[6 * Geo<ORDER>::PL + h + Geo<ORDER>::W] - pm[6 * Geo<ORDER>::PL + h - Geo<ORDER>::W]) / (2. * B.dy) +
+                              (pu[7 * Geo<ORDER>::PL + h] - bz_below) / (2. * B.dz);
+          const double v1 = pm[1 * Geo<ORDER>::PL + h], v2 = pm[2 * Geo<ORDER>::PL + h], v3 = pm[3 * Geo<ORDER>::PL + h];
+          const double b1 = pm[5 * Geo<ORDER>::PL + h], b2 = pm[6 * Geo<ORDER>::PL + h], b3 = pm[7 * Geo<ORDER>::PL + h];
           s[1] = -divB * b1;
           s[2] = -divB * b2;
           s[3] = -divB * b3;
@@ -263,8 +338,9 @@ __global__ void __launch_bounds__(STAGE_THREADS, (!MHD && NEQ == 5) ? 2 : 1) sta
           s[6] = -divB * v2;
           s[7] = -divB * v3;
         }
-        if (MHD) bz_below = ring[ring_slot(m) * CH * HPLANE + 7 * HPLANE + hc];
+        if (MHD) bz_below = ring[ring_slot(m) * CH * Geo<ORDER>::PL + 7 * Geo<ORDER>::PL + hc];
         const size_t o = cell_off(slot, NEQ, 0, ci, cj, m);
+        double wv[NEQ];
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) {
           const double fxl = fxs[(e * NC + (cj - 1)) * 17 + ci - 1], fxr = fxs[(e * NC + (cj - 1)) * 17 + ci];
@@ -272,15 +348,52 @@ __global__ void __launch_bounds__(STAGE_THREADS, (!MHD && NEQ == 5) ? 2 : 1) sta
           double v = __ldg(P.base + o + (size_t)e * BCELLS) + dtdx * (fxl - fxr) + dtdy * (fyl - fyr) +
                      dtdz * (zprev[e] - znew[e]);
           if (MHD && ph.eight_wave) v = v + dtp * s[e];
-          P.out[o + (size_t)e * BCELLS] = v;
+          if (VISC) wv[e] = v;
+          else P.out[o + (size_t)e * BCELLS] = v;
+        }
+        if constexpr (VISC) {
+          double* wb = wpl + (m & 1) * NEQ * VPLANE;          // W(m-2) of the column, then W(m)
+          const double* wc = wpl + ((m - 1) & 1) * NEQ * VPLANE;  // W(m-1) with its frame
+          if (m > z0) {
+            double un[NEQ];
+#pragma unroll
+            for (int e = 0; e < NEQ; ++e) {
+              const double* pe = wc + e * VPLANE;
+              const double c = pe[vq(ci, cj)];
+              un[e] = c + ph.eta * (+pe[vq(ci + 1, cj)] + pe[vq(ci - 1, cj)] + pe[vq(ci, cj + 1)] + pe[vq(ci, cj - 1)] +
+                                    wv[e] + wb[e * VPLANE + vq(ci, cj)] - 6.0 * c);
+            }
+            visc_store<NEQ, MHD>(P, B, un, o - NC * NC, dtl, nonfinite);
+          }
+#pragma unroll
+          for (int e = 0; e < NEQ; ++e) wb[e * VPLANE + vq(ci, cj)] = wv[e];
         }
       }
 #pragma unroll
       for (int e = 0; e < NEQ; ++e) zprev[e] = znew[e];
       __syncthreads();
     }
+    if (VISC && t < PLANE) {  // viscous step of plane z1: above it, the top UP ghost
+      double g[NEQ], un[NEQ];
+      gather_ghost<NEQ>(P.src, B, slot, ci, cj, z1 + 1, g);
+      const double* wc = wpl + (z1 & 1) * NEQ * VPLANE;
+      const double* wb = wpl + ((z1 - 1) & 1) * NEQ * VPLANE;
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e) {
+        const double* pe = wc + e * VPLANE;
+        const double c = pe[vq(ci, cj)];
+        un[e] = c + ph.eta * (+pe[vq(ci + 1, cj)] + pe[vq(ci - 1, cj)] + pe[vq(ci, cj + 1)] + pe[vq(ci, cj - 1)] + g[e] +
+                              wb[e * VPLANE + vq(ci, cj)] - 6.0 * c);
+      }
+      visc_store<NEQ, MHD>(P, B, un, cell_off(slot, NEQ, 0, ci, cj, z1), dtl, nonfinite);
+    }
   }
   flush_counts(P.ctl, pf, df, zd);
+  if (VISC) {
+    if (P.do_dt) block_min_dt(dtl, P.ctl);
+    nonfinite = __reduce_add_sync(0xffffffffu, nonfinite);
+    if ((t & 31) == 0 && nonfinite) atomicAdd(&P.ctl->cnt[3], (unsigned long long)nonfinite);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -355,15 +468,6 @@ struct ViscParams {
   DevCtl* ctl;
   PhysParams ph;
 };
-
-__device__ __forceinline__ void block_min_dt(double v, DevCtl* ctl) {
-  v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 16));
-  v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 8));
-  v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 4));
-  v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 2));
-  v = fmin(v, __shfl_xor_sync(0xffffffffu, v, 1));
-  if ((threadIdx.x & 31) == 0) atomic_min_pos(&ctl->dtmin_bits, v);
-}
 
 template <int NEQ, bool MHD>
 __global__ void __launch_bounds__(256) viscous_kernel(ViscParams P) {

@@ -86,13 +86,19 @@ class Walicxe3D:
     def set_zsplit(self, z: int):
         self._chk(self.lib.wx3d_set_zsplit(self.ctx, int(z)), "wx3d_set_zsplit")
 
+    def set_fusion(self, on: bool):
+        self._chk(self.lib.wx3d_set_fusion(self.ctx, int(bool(on))), "wx3d_set_fusion")
+
+    SHAPES = ("1-fused", "1", "2", "4", "8")
+
     def autotune(self, reps: int = 3):
-        """Measured choice of the stage launch shape (z-slab split) for the
-        current mesh; returns (chosen split, {split: ms per predictor+corrector pass})."""
-        ms = (ctypes.c_double * 4)()
-        best = ctypes.c_int32()
-        self._chk(self.lib.wx3d_autotune(self.ctx, int(reps), ms, ctypes.byref(best)), "wx3d_autotune")
-        return best.value, dict(zip((1, 2, 4, 8), list(ms)))
+        """Measured choice of the stage launch shape (z-slab split, and for
+        whole blocks whether the corrector carries the viscous step) for the
+        current mesh; returns (split, fused, {shape: ms per solver pass})."""
+        ms = (ctypes.c_double * 5)()
+        best = (ctypes.c_int32 * 2)()
+        self._chk(self.lib.wx3d_autotune(self.ctx, int(reps), ms, best), "wx3d_autotune")
+        return best[0], bool(best[1]), dict(zip(self.SHAPES, list(ms)))
 
     def neighbours(self):
         n = self.nslots
