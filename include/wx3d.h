@@ -328,6 +328,10 @@ int wx3d_set_surrogate(wx_ctx* ctx, wx_mlp* mlp, const uint8_t* trust, int32_t n
  * over the n positive normal arguments host_x. */
 int wx3d_check_fast_math(int32_t n, const double* host_x, int64_t* max_ulp2);
 
+/* Measured FP64 FMA throughput of the current device in GFLOP/s (an FMA
+ * counts two flops): the compute roofline of the stage kernels. */
+int wx3d_measure_fp64_peak(double* gflops);
+
 /* Human-readable text of a status code and of the context's last error. */
 const char* wx3d_error_string(int32_t code);
 int wx3d_last_error(wx_ctx* ctx, char* buf, int32_t len);

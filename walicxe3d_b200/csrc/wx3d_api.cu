@@ -420,6 +420,21 @@ void invalidate_graph(wx_ctx* c) {
 
 bool ready(wx_ctx* c) { return c && c->nwork > 0; }
 
+// FP64 FMA throughput: 8 independent chains per thread, 4096 steps each.
+__global__ void __launch_bounds__(256) fp64_peak_kernel(double* out, double a, double b) {
+  double x[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) x[i] = threadIdx.x * 1e-3 + i;
+  for (int s = 0; s < 4096; ++s) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = fma(x[i], a, b);
+  }
+  double r = 0.0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) r += x[i];
+  if (r == 12345.678) out[0] = r;  // keeps the chains live
+}
+
 __device__ __forceinline__ unsigned long long ulp_dist(double a, double b) {
   const long long x = __double_as_longlong(a), y = __double_as_longlong(b);
   return (unsigned long long)(x > y ? x - y : y - x);
@@ -1059,6 +1074,39 @@ int wx3d_kernel_times(wx_ctx* c, double* ms4, int32_t* count4) {
     ms4[k] += ms;
     if (count4) ++count4[k];
   }
+  return WX_OK;
+}
+
+// Measured FP64 FMA throughput of the device (GFLOP/s, one FMA = 2 flops):
+// the compute roofline of the stage kernels, which are bound by FP64 issue.
+int wx3d_measure_fp64_peak(double* gflops) {
+  if (!gflops) return WX_ERR_INVALID_ARG;
+  int ndev = 0, dev = 0, nsm = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return WX_ERR_NO_DEVICE;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  double* d = nullptr;
+  if (cudaMalloc(&d, 8) != cudaSuccess) return WX_ERR_CUDA;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int grid = nsm * 8;
+  float best = 1e30f;
+  for (int r = 0; r < 6; ++r) {
+    cudaEventRecord(e0);
+    fp64_peak_kernel<<<grid, 256>>>(d, 0.999999, 1e-7);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r > 0 && ms < best) best = ms;
+  }
+  const cudaError_t e = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d);
+  if (e != cudaSuccess) return WX_ERR_CUDA;
+  *gflops = 2.0 * 8.0 * 4096.0 * 256.0 * grid / (best * 1e-3) / 1e9;
   return WX_OK;
 }
 

@@ -279,8 +279,11 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
     for (int m = z0; m <= z1; ++m) {
       // ---- phase A: load plane m+ORDER+1; z-flux m+1/2; x/y fluxes of m ---
       if (m + ORDER + 1 <= z1 + ORDER) load_plane<NEQ, MHD, ORDER, CH>(P, B, slot, m + ORDER + 1, z0, z1, ring, pf, df, zd);
-      if (VISC && t >= PLANE) {  // one-deep x/y frame of W(m): UP ghosts of plane m
-        for (int f = t - PLANE; f < 4 * NC; f += STAGE_THREADS - PLANE) {
+      // one-deep x/y frame of W(m): UP ghosts of plane m, on threads 96..159,
+      // which load a single ring cell per plane (threads below 96 load two)
+      if (VISC && t >= 96 && t < 96 + 4 * NC) {
+        {
+          const int f = t - 96;
           const int side = f >> 4, r = (f & 15) + 1;
           const int gi = side == 0 ? 0 : (side == 1 ? NC + 1 : r);
           const int gj = side == 2 ? 0 : (side == 3 ? NC + 1 : r);
