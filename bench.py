@@ -134,17 +134,25 @@ def cpu_time_oracle(prob, steps_max: int, budget_s: float, threads: int):
     return prob.cells * n / dt / 1e6, n, dt
 
 
-def load_traffic(workload: str, cells_per_launch: int):
-    """DRAM bytes per launch of the corrector stage from the committed ncu
-    summary (bytes per cell measured on a smaller case), scaled to the launch."""
-    f = ROOT / "profiles" / "stage2_traffic.json"
-    if not f.exists():
+def stage_figures(neq: int, fused: bool):
+    """Per-cell DRAM bytes and FP64 flops of the corrector from the committed
+    ncu summary (profiles/stage_kernels.json, measured on Sedov 256^3 at
+    neq 5); None for other equation counts, which that capture does not
+    cover."""
+    f = ROOT / "profiles" / "stage_kernels.json"
+    if neq != 5 or not f.exists():
         return None
     try:
         d = json.loads(f.read_text())
-        return d["dram_bytes_per_cell"] * cells_per_launch
+        return d["corrector_fused" if fused else "corrector"]
     except Exception:
         return None
+
+
+def fp64_peak_tflops(lib):
+    import ctypes
+    g = ctypes.c_double()
+    return g.value / 1e3 if lib.wx3d_measure_fp64_peak(ctypes.byref(g)) == 0 else None
 
 
 def run_reference(args, rank, world):
@@ -278,11 +286,21 @@ def main():
         peak, peak_src = 6650.0, "fallback"
     neq = prob.cfg.neqtot
     stage2_ms = kt_ms[1] / max(kt_n[1], 1)
+    fused = kt_n[2] == 0          # no separate viscous launch: the corrector carries it
     alg_bytes = 3 * neq * 8 * prob.cells     # reads UP and U, writes the stage result
     achieved = alg_bytes / (stage2_ms / 1e3) / 1e9 if stage2_ms > 0 else None
     step_bytes = 40 * neq * prob.cells       # 5 compulsory state passes per step
     step_achieved = step_bytes * args.steps * world / (ms / 1e3) / 1e9
-    traffic = load_traffic(args.workload, prob.cells)
+    fig = stage_figures(neq, fused)
+    traffic = fig["dram_bytes_per_cell"] * prob.cells if fig else None
+    fp64 = None
+    if fig and "fp64_flops_per_cell" in fig and stage2_ms > 0:
+        pk = fp64_peak_tflops(w.lib)
+        ach = fig["fp64_flops_per_cell"] * prob.cells / (stage2_ms / 1e3) / 1e12
+        fp64 = {"achieved_tflops": ach, "peak_tflops": pk, "frac": (ach / pk) if pk else None,
+                "flops_per_cell": fig["fp64_flops_per_cell"],
+                "peak_source": "measured in this run (wx3d_measure_fp64_peak, DFMA chains)",
+                "note": "the stage kernels are bound by FP64 issue, not by HBM"}
 
     # --- end to end through the C-ABI with host buffers ---
     U_host = torch.from_numpy(prob.U).pin_memory()
@@ -334,7 +352,8 @@ def main():
                                               "ms_per_pass": tuned["ms_per_pass"]}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                         "kernel": "stage_kernel<ORDER=2> (corrector)", "peak_source": peak_src,
+                         "kernel": "stage_kernel<ORDER=2> (corrector%s)" % (" + viscous step" if fused else ""),
+                         "peak_source": peak_src, "fp64": fp64,
                          "alg_bytes_per_launch": alg_bytes, "launch_ms": stage2_ms,
                          "step_alg_gbs": step_achieved, "step_frac": step_achieved / peak},
             "kernel_ms_per_launch": {k: (m / n if n else None) for k, m, n in
