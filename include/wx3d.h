@@ -170,6 +170,23 @@ int wx3d_get_neighbours(wx_ctx* ctx, int32_t nslots, int32_t* face_type, int32_t
  * wx3d_set_mesh picks a default; the autotuner overrides it. */
 int wx3d_set_zsplit(wx_ctx* ctx, int32_t zsplit);
 
+/* A spherical wind source (spherical_wind_type, winds.f90), physical cgs
+ * units: centre, bulk velocity of the source, radius, mass-loss rate,
+ * terminal speed, temperature, mean molecular mass.  y0 is the neutral
+ * fraction of the wind's passive scalar (EOS_H_RATE runs), a value the
+ * reference leaves undefined. */
+typedef struct wx_wind {
+  double xc, yc, zc, vx, vy, vz, radius, mdot, vinf, temp, mu, y0;
+} wx_wind;
+
+/* userBoundary hook of the wind problems (imposeSphericalWind,
+ * winds.f90:123-240): after every ghost exchange the reference re-imposes
+ * the r^-2 wind in all cells, ghosts included, within a source's radius.
+ * The library applies it where the stages read those cells.  nwind = 0
+ * removes the sources.  The zone refinement the reference does at it = 0
+ * (refineZone) is the host's, like the rest of the mesh. */
+int wx3d_set_winds(wx_ctx* ctx, int32_t nwind, const wx_wind* winds);
+
 /* With fusion on (the default) and whole blocks per CTA (zsplit 1), the
  * corrector stage also applies doViscousStep; otherwise a separate viscous
  * kernel runs after it.  The autotuner overrides the choice. */

@@ -418,3 +418,33 @@ def test_autotune_picks_a_shape_and_keeps_the_state():
     assert z in (1, 2, 4, 8) and set(ms) == set(g.SHAPES) and all(v > 0 for v in ms.values())
     assert fused in (True, False)
     assert np.array_equal(g.download(), U0)
+
+
+@pytest.mark.parametrize("shape", ["default", "1-fused"])
+def test_colliding_winds_match_oracle(shape, ncpu):
+    """Two spherical wind sources re-imposed before each stage (the
+    userBoundary hook, winds.f90:123-240) with table cooling, on a
+    two-level mesh, against the CPU oracle."""
+    prob = problems.colliding_winds(nroot=2, maxlev=3, r_wind_pc=0.12)
+    o = oracle.from_problem(prob, threads=ncpu)
+    g = from_problem(prob)
+    if shape != "default":
+        _shape(g, shape)
+    for _ in range(6):
+        o.step()
+        g.step()
+    check(o, g, prob)
+
+
+def test_wind_sphere_on_a_level_transition_is_refused():
+    """A sphere that reaches the ghost layer of a coarse/fine face would need
+    the wind at ghost positions no same-level neighbour provides: refused."""
+    from walicxe3d_b200._lib import WxError
+    prob = problems.colliding_winds(nroot=2, maxlev=3, r_wind_pc=0.12)
+    g = from_problem(prob)
+    L = prob.cfg.box[0]
+    bad = [[0.2 * L, 0.5 * L, 0.5 * L, 0, 0, 0, 0.3 * L, 1e20, 1e8, 1e5, 0.61, 0.0]]
+    with pytest.raises(WxError) as e:
+        g.set_winds(bad)
+    assert e.value.code == 104
+    g.step()   # the previous sources stay in force

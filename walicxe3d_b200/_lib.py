@@ -30,6 +30,7 @@ _SIGNATURES = {
     "wx3d_set_mesh": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_int32_p]),
     "wx3d_set_zsplit": (ctypes.c_int, [c_void_p, ctypes.c_int32]),
     "wx3d_set_fusion": (ctypes.c_int, [c_void_p, ctypes.c_int32]),
+    "wx3d_set_winds": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_double_p]),
     "wx3d_autotune": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_double_p, c_int32_p]),
     "wx3d_get_neighbours": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_int32_p, c_int32_p]),
     "wx3d_upload_blocks": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_double_p]),

@@ -34,6 +34,7 @@ struct Kern {
   void (*lax)(LaxParams) = nullptr;
   void (*visc)(ViscParams) = nullptr;
   void (*dt)(DtParams) = nullptr;
+  void (*wind)(WindParams) = nullptr;
   void (*src)(SrcParams) = nullptr;
   void (*mark)(MarkParams) = nullptr;
   void (*prims)(const double*, double*, const int32_t*, int, DevCtl*, double) = nullptr;
@@ -51,6 +52,7 @@ Kern make_kern() {
   k.lax = lax_kernel<NEQ, MHD>;
   k.visc = viscous_kernel<NEQ, MHD>;
   k.dt = dt_kernel<NEQ, MHD>;
+  k.wind = wind_kernel<NEQ, MHD>;
   k.src = source_kernel<NEQ, MHD>;
   k.mark = mark_kernel<NEQ, MHD>;
   k.prims = prims_kernel<NEQ, MHD>;
@@ -163,6 +165,8 @@ struct wx_ctx {
   std::vector<int32_t> local;     // localBlocks
   std::vector<int32_t> work;      // occupied slots
   std::vector<DevBlock> hblocks;
+  std::vector<double> hwind;      // wind sources, 12 doubles each (wx_wind)
+  double* dWind = nullptr;
   int nwork = 0;
   int zsplit = 1;
   bool fuse = true;   // corrector carries the viscous step when zsplit == 1
@@ -251,6 +255,67 @@ void fill_phys(wx_ctx* c) {
   p.cooling = f.cooling_type;
   p.fp = 5 + 3 * (f.bfield ? 1 : 0);
   p.npassive = f.npassive;
+  p.l_sc = f.l_sc;
+  p.v_sc = f.v_sc;
+  p.wind = c->dWind;
+  p.nwind = (int32_t)(c->hwind.size() / 12);
+}
+
+// Flags the blocks whose cells, ghost layers included, a wind sphere
+// reaches (cell centres from cellPos, amr.f90:1037-1065).  Returns false
+// (with the slot in *bad) if a sphere reaches the ghost layer of a face
+// with a coarser or finer neighbour: those ghosts would need the wind at
+// their own positions (or their sources the values before it), which only
+// a same-level neighbour provides.
+bool flag_wind_blocks(const wx_ctx* c, std::vector<DevBlock>& hb, int* bad) {
+  const size_t nw = c->hwind.size() / 12;
+  const double l_sc = c->cfg.l_sc;
+  auto reach = [&](const double* W, const double* lo, const double* hi) {
+    double s = 0.0;
+    for (int ax = 0; ax < 3; ++ax) {
+      const double q = W[ax] < lo[ax] ? lo[ax] - W[ax] : (W[ax] > hi[ax] ? W[ax] - hi[ax] : 0.0);
+      s += q * q;
+    }
+    return std::sqrt(s) <= W[6] * (1.0 + 1e-12);
+  };
+  for (size_t s = 0; s < hb.size(); ++s) {
+    DevBlock& b = hb[s];
+    b.wind = 0;
+    if (b.level < 1 || nw == 0) continue;
+    const double d[3] = {b.dx, b.dy, b.dz};
+    double lo[3], hi[3];
+    for (int ax = 0; ax < 3; ++ax) {   // cells -1 .. 18 (their volumes)
+      lo[ax] = ((b.bc[ax] - 1) * NC - 2) * d[ax] * l_sc;
+      hi[ax] = ((b.bc[ax] - 1) * NC + 18) * d[ax] * l_sc;
+    }
+    for (size_t w = 0; w < nw; ++w) {
+      const double* W = &c->hwind[12 * w];
+      if (!reach(W, lo, hi)) continue;
+      b.wind = 1;
+      for (int f = 0; f < 6; ++f) {
+        if (b.ftype[f] != WX_NEIGH_COARSER && b.ftype[f] != WX_NEIGH_FINER) continue;
+        const int ax = f / 2, side = f & 1;
+        double glo[3], ghi[3];
+        // the volume of the face's two ghost layers: it holds the ghost
+        // centres and every neighbour cell a coarse/fine ghost is made from
+        for (int a2 = 0; a2 < 3; ++a2) {
+          const double base = (b.bc[a2] - 1) * NC;
+          if (a2 == ax) {
+            glo[a2] = (side ? base + 16 : base - 2) * d[a2] * l_sc;
+            ghi[a2] = (side ? base + 18 : base) * d[a2] * l_sc;
+          } else {
+            glo[a2] = base * d[a2] * l_sc;
+            ghi[a2] = (base + 16) * d[a2] * l_sc;
+          }
+        }
+        if (reach(W, glo, ghi)) {
+          if (bad) *bad = (int)s;
+          return false;
+        }
+      }
+    }
+  }
+  return true;
 }
 
 bool sources_on(const wx_ctx* c) { return c->cfg.eos_type == WX_EOS_H_RATE || c->cfg.cooling_type != WX_COOL_NONE; }
@@ -294,11 +359,19 @@ int launch_dt(wx_ctx* c, const double* u) {
   return WX_OK;
 }
 
+int launch_wind(wx_ctx* c, double* u) {
+  if (c->hwind.empty()) return WX_OK;
+  WindParams P{u, c->dBlocks, c->dWork, c->nwork, c->ph};
+  c->k.wind<<<grid_for(c, (const void*)c->k.wind, 256, 0, c->nwork), 256, 0, c->stream>>>(P);
+  WX_LAUNCHED();
+  return WX_OK;
+}
+
 // fused: the corrector that also applies doViscousStep (whole blocks only)
 int launch_stage(wx_ctx* c, int order, const double* src, const double* base, double* out, double factor,
-                 bool fused = false) {
+                 bool fused = false, const double* gsrc = nullptr) {
   StageParams P{src, base, out, c->dBlocks, c->dWork, c->nwork * c->zsplit, c->zsplit, c->dCtl, factor, c->ph,
-                sources_on(c) ? 0 : 1};
+                sources_on(c) ? 0 : 1, gsrc ? gsrc : src};
   auto fn = order == 1 ? c->k.stage1 : (fused ? c->k.stage2v : c->k.stage2);
   const size_t smem = order == 1 ? c->k.smem1 : (fused ? c->k.smem2v : c->k.smem2);
   const int grid = grid_for(c, (const void*)fn, STAGE_THREADS, smem, c->nwork * c->zsplit);
@@ -310,9 +383,10 @@ int launch_stage(wx_ctx* c, int order, const double* src, const double* base, do
   return WX_OK;
 }
 
-// doViscousStep on dW in place, UP ghosts (zero for single-stage solvers)
-int launch_visc(wx_ctx* c, int zero_ghost) {
-  ViscParams V{c->dW, c->dUP, c->dBlocks, c->dWork, c->nwork, zero_ghost, sources_on(c) ? 0 : 1, c->dCtl, c->ph};
+// doViscousStep in place on w (the stage result), UP ghosts (zero for
+// single-stage solvers)
+int launch_visc(wx_ctx* c, int zero_ghost, double* w = nullptr) {
+  ViscParams V{w ? w : c->dW, c->dUP, c->dBlocks, c->dWork, c->nwork, zero_ghost, sources_on(c) ? 0 : 1, c->dCtl, c->ph};
   tick(c, 2, true);
   c->k.visc<<<grid_for(c, (const void*)c->k.visc, 256, 0, c->nwork), 256, 0, c->stream>>>(V);
   WX_LAUNCHED();
@@ -335,6 +409,27 @@ int enqueue_solver(wx_ctx* c, bool bump_it, bool finish_output) {
   WX_LAUNCHED();
   int zero_ghost = 0;
   int rc;
+  if (!c->hwind.empty()) {
+    // Wind run (userBoundary after every ghost fill, winds.f90:123-240).
+    // Stage 1 of godunov.f90 refreshes only the ghost primitives after
+    // boundary(1, U): the physical cells feed their fluxes with the
+    // primitives of U before the wind, the ghosts see it.  So the physical
+    // cells come from U and the ghosts from a wind-imposed copy of U in W,
+    // which is also the base of stage 2; boundary(2, UP) imposes the wind on
+    // UP's physical cells.  The result goes to U (no swap).
+    WX_CUDA(cudaMemcpyAsync(c->dW, c->dU, sizeof(double) * (size_t)c->max_blocks * c->neq * BCELLS,
+                            cudaMemcpyDeviceToDevice, c->stream));
+    if ((rc = launch_wind(c, c->dW))) return rc;
+    if ((rc = launch_stage(c, 1, c->dU, c->dU, c->dUP, 0.5, false, c->dW))) return rc;
+    if ((rc = launch_wind(c, c->dUP))) return rc;
+    if ((rc = launch_stage(c, 2, c->dUP, c->dW, c->dU, 1.0, fuse_visc(c)))) return rc;
+    if (!fuse_visc(c) && (rc = launch_visc(c, 0, c->dU))) return rc;
+    step_end_kernel<<<1, 1, 0, c->stream>>>(c->dCtl, finish_output ? 1 : 0);
+    WX_LAUNCHED();
+    c->prestep = true;
+    c->dt_valid = !src;
+    return WX_OK;
+  }
   if (solver == WX_SOLVER_LAX) {
     LaxParams P{c->dU, c->dW, c->dBlocks, c->dWork, c->nwork, c->dCtl, c->ph};
     tick(c, 1, true);
@@ -555,6 +650,7 @@ int wx3d_finalize(wx_ctx* c) {
   cudaFree(c->dU); cudaFree(c->dUP); cudaFree(c->dW); cudaFree(c->dPrim); cudaFree(c->dStage);
   cudaFree(c->dBlocks); cudaFree(c->dWork); cudaFree(c->dFlags); cudaFree(c->dCtl); cudaFree(c->dCool);
   cudaFree(c->dTrust);
+  cudaFree(c->dWind);
   if (c->hCtl) cudaFreeHost(c->hCtl);
   for (int i = 0; i < 64; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -642,6 +738,10 @@ int wx3d_set_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb) {
   }
   c->local.assign(c->max_blocks, -1);
   std::copy(lb, lb + nslots, c->local.begin());
+  int bad = -1;
+  if (!flag_wind_blocks(c, hb, &bad))
+    return fail(c, WX_ERR_UNSUPPORTED, "slot %d: a wind sphere reaches the ghost layer of a coarse/fine face; "
+                "refine the zone around the source (refineZone) further", bad);
   c->hblocks = hb;
   c->work = work;
   c->nwork = (int)work.size();
@@ -668,6 +768,47 @@ int wx3d_set_zsplit(wx_ctx* c, int32_t zsplit) {
 // Measured choice of the z-slab split: times the predictor and corrector
 // stages (which write only the UP and W scratch arrays, so U and the
 // simulation state are untouched) for every split and keeps the fastest.
+// userBoundary hook of the wind problems (imposeSphericalWind,
+// winds.f90:123-240): nwind sources in physical (cgs) units; 0 removes them.
+int wx3d_set_winds(wx_ctx* c, int32_t nwind, const wx_wind* winds) {
+  if (!c || nwind < 0 || (nwind > 0 && !winds)) return WX_ERR_INVALID_ARG;
+  if (nwind > 0 && (c->cfg.solver_type == WX_SOLVER_LAX || c->cfg.solver_type == WX_SOLVER_HLL1))
+    return fail(c, WX_ERR_UNSUPPORTED, "wind sources with a single-stage solver");
+  if (nwind > 0 && c->cfg.npassive > 1)
+    return fail(c, WX_ERR_UNSUPPORTED, "wind sources with more than one passive scalar (the reference leaves them undefined)");
+  std::vector<double> h((size_t)nwind * 12);
+  for (int w = 0; w < nwind; ++w) {
+    const wx_wind& s = winds[w];
+    const double v[12] = {s.xc, s.yc, s.zc, s.vx, s.vy, s.vz, s.radius, s.mdot, s.vinf, s.temp, s.mu, s.y0};
+    if (!(s.radius > 0.0) || !(s.vinf > 0.0) || !(s.mdot > 0.0) || !(s.mu > 0.0))
+      return fail(c, WX_ERR_INVALID_ARG, "wind %d: radius, vinf, mdot and mu must be positive", w);
+    std::copy(v, v + 12, h.begin() + 12 * w);
+  }
+  std::vector<double> prev = c->hwind;
+  c->hwind = h;
+  int bad = -1;
+  std::vector<DevBlock> hb = c->hblocks;
+  if (!flag_wind_blocks(c, hb, &bad)) {
+    c->hwind = prev;
+    return fail(c, WX_ERR_UNSUPPORTED, "slot %d: a wind sphere reaches the ghost layer of a coarse/fine face; "
+                "refine the zone around the source (refineZone) further", bad);
+  }
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  cudaFree(c->dWind);
+  c->dWind = nullptr;
+  if (nwind > 0) {
+    WX_CUDA(cudaMalloc(&c->dWind, sizeof(double) * h.size()));
+    WX_CUDA(cudaMemcpy(c->dWind, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+  }
+  c->hblocks = hb;
+  fill_phys(c);
+  WX_CUDA(cudaMemcpyAsync(c->dBlocks, c->hblocks.data(), sizeof(DevBlock) * c->max_blocks, cudaMemcpyHostToDevice,
+                          c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  invalidate_graph(c);
+  return WX_OK;
+}
+
 int wx3d_set_fusion(wx_ctx* c, int32_t on) {
   if (!c) return WX_ERR_INVALID_ARG;
   c->fuse = on != 0;
@@ -1324,6 +1465,8 @@ void noalloc_phys(const wx_config& f, PhysParams& p) {
   p.cooling = f.cooling_type;
   p.fp = 5 + 3 * (f.bfield ? 1 : 0);
   p.npassive = f.npassive;
+  p.l_sc = f.l_sc;
+  p.v_sc = f.v_sc;
 }
 
 int noalloc_grid(const void* fn, int threads, size_t smem, int items, int nsm) {

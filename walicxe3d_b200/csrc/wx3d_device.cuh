@@ -30,6 +30,7 @@ struct __align__(16) DevBlock {
   int32_t ftype[6];    // WX_NEIGH_* per face (LEFT..TOP), 0 = empty slot
   int32_t fnb[6][4];   // neighbour slots: [0] for SAME/COARSER, [0..3] for FINER;
                        // for BOUNDARY faces fnb[f][0] holds the BC type
+  int32_t wind;        // 1: a wind sphere reaches the block or its ghost cells
   double dx, dy, dz;   // cell size at this level (init.f90:726-730)
 };
 
@@ -61,6 +62,9 @@ struct PhysParams {
   int32_t cooling;
   int32_t fp;        // 0-based first passive
   int32_t npassive;
+  double l_sc, v_sc;
+  const double* wind;  // nwind x 12: xc yc zc vx vy vz radius mdot vinf temp mu y0 (cgs)
+  int32_t nwind;
 };
 
 // ---------------------------------------------------------------------------

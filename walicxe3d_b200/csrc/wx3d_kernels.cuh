@@ -9,6 +9,7 @@
 #pragma once
 
 #include "wx3d_device.cuh"
+#include "wx3d_wind.cuh"
 
 namespace wx {
 
@@ -16,7 +17,7 @@ constexpr int STAGE_THREADS = 288;  // 17*16 x- and y-interfaces per plane
 constexpr int RING = 4;             // planes p-1..p+2 of the second-order stencil
 
 struct StageParams {
-  const double* __restrict__ src;   // array whose primitives feed the fluxes
+  const double* __restrict__ src;   // array whose primitives feed the fluxes (physical cells)
   const double* __restrict__ base;  // array the update starts from (U)
   double* __restrict__ out;         // result (UP for stage 1, W for stage 2)
   const DevBlock* __restrict__ blocks;
@@ -27,6 +28,8 @@ struct StageParams {
   double dt_factor;                 // 0.5 for the predictor, 1 otherwise
   PhysParams ph;
   int32_t do_dt;                    // fused viscous step: fold the CFL minimum of the result
+  const double* __restrict__ gsrc;  // array the ghost cells are gathered from (src, or the
+                                    // wind-imposed copy of U in the first stage of a wind run)
 };
 
 // Ring plane geometry: 16x16 cells with the ORDER-deep x/y ghost frame.
@@ -181,8 +184,8 @@ __device__ __forceinline__ void load_plane(const StageParams& P, const DevBlock&
       else { i = r; j = NC + 2 - d; }
     }
     double u[NEQ], p[NEQ], rinv;
-    if (inner) get_cell<NEQ>(P.src, B, slot, i, j, kk, u);
-    else gather_ghost<NEQ>(P.src, B, slot, i, j, kk, u);
+    if (inner && c < PLANE) load_cell<NEQ>(P.src, slot, i, j, kk, u);
+    else gather_ghost<NEQ>(P.gsrc, B, slot, i, j, kk, u);
     const int st = flow2prim<NEQ, MHD>(u, p, ph.cv, &rinv);
     if constexpr (CH > NEQ) {
       pl[NEQ * Geo<ORDER>::PL + hidx<ORDER>(i, j)] = sqrt_nr(ph.gamma * p[4] * rinv);
@@ -612,6 +615,39 @@ __global__ void step_end_kernel(DevCtl* ctl, int finish_output) {
     ctl->nextout = ctl->nextout + 1;
     ctl->dumpout = 0;
     ctl->dumps = ctl->dumps + 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// userBoundary of the wind problems: imposes the wind on the physical cells
+// of `u` inside the spheres (blocks flagged in the neighbour table only).
+// A ghost in a sphere is then gathered from a same-level neighbour whose
+// cell at the same position carries the same imposed value
+// (wx3d_set_winds refuses meshes where a coarse/fine face's ghost layer
+// meets a sphere).
+struct WindParams {
+  double* __restrict__ u;
+  const DevBlock* __restrict__ blocks;
+  const int32_t* __restrict__ work;
+  int32_t nwork;
+  PhysParams ph;
+};
+
+template <int NEQ, bool MHD>
+__global__ void __launch_bounds__(256) wind_kernel(WindParams P) {
+  for (int w = blockIdx.x; w < P.nwork; w += gridDim.x) {
+    const int slot = P.work[w];
+    const DevBlock& B = P.blocks[slot];
+    if (!B.wind) continue;
+    for (int c = threadIdx.x; c < BCELLS; c += blockDim.x) {
+      const int i = (c & 15) + 1, j = ((c >> 4) & 15) + 1, k = (c >> 8) + 1;
+      double u[NEQ];
+      if (wind_state<NEQ, MHD>(P.ph, B, i, j, k, u)) {
+        const size_t o = cell_off(slot, NEQ, 0, i, j, k);
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) P.u[o + (size_t)e * BCELLS] = u[e];
+      }
+    }
   }
 }
 

@@ -86,6 +86,14 @@ class Walicxe3D:
     def set_zsplit(self, z: int):
         self._chk(self.lib.wx3d_set_zsplit(self.ctx, int(z)), "wx3d_set_zsplit")
 
+    def set_winds(self, winds):
+        """Spherical wind sources (rows of 12: xc yc zc vx vy vz radius mdot
+        vinf temp mu y0, cgs), re-imposed after every ghost exchange as the
+        reference's userBoundary does."""
+        w = np.ascontiguousarray(np.asarray(winds, dtype=np.float64).reshape(-1, 12))
+        self._chk(self.lib.wx3d_set_winds(self.ctx, len(w), w.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                  "wx3d_set_winds")
+
     def set_fusion(self, on: bool):
         self._chk(self.lib.wx3d_set_fusion(self.ctx, int(bool(on))), "wx3d_set_fusion")
 
@@ -258,6 +266,8 @@ def from_problem(prob, extra_slots: int = 0) -> Walicxe3D:
     w.upload(prob.U)
     if prob.cooltable is not None:
         w.set_cooltable(*prob.cooltable)
+    if prob.winds:
+        w.set_winds(prob.winds)
     w.set_state(time=0.0, dt=0.0, it=0, nextout=1)
     return w
 
