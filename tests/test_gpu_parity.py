@@ -423,9 +423,9 @@ def test_autotune_picks_a_shape_and_keeps_the_state():
 @pytest.mark.parametrize("shape", ["default", "1-fused"])
 def test_colliding_winds_match_oracle(shape, ncpu):
     """Two spherical wind sources re-imposed before each stage (the
-    userBoundary hook, winds.f90:123-240) with table cooling, on a
-    two-level mesh, against the CPU oracle."""
-    prob = problems.colliding_winds(nroot=2, maxlev=3, r_wind_pc=0.12)
+    userBoundary hook, winds.f90:123-240) with EOS_H_RATE and table
+    cooling, on a two-level mesh, against the CPU oracle."""
+    prob = problems.colliding_winds(nroot=2, maxlev=3, r_wind_cells=8)
     o = oracle.from_problem(prob, threads=ncpu)
     g = from_problem(prob)
     if shape != "default":
@@ -440,7 +440,7 @@ def test_wind_sphere_on_a_level_transition_is_refused():
     """A sphere that reaches the ghost layer of a coarse/fine face would need
     the wind at ghost positions no same-level neighbour provides: refused."""
     from walicxe3d_b200._lib import WxError
-    prob = problems.colliding_winds(nroot=2, maxlev=3, r_wind_pc=0.12)
+    prob = problems.colliding_winds(nroot=2, maxlev=3, r_wind_cells=8)
     g = from_problem(prob)
     L = prob.cfg.box[0]
     bad = [[0.2 * L, 0.5 * L, 0.5 * L, 0, 0, 0, 0.3 * L, 1e20, 1e8, 1e5, 0.61, 0.0]]
@@ -448,3 +448,29 @@ def test_wind_sphere_on_a_level_transition_is_refused():
         g.set_winds(bad)
     assert e.value.code == 104
     g.step()   # the previous sources stay in force
+
+
+def test_small_wind_sphere_fails_at_the_same_step_as_the_reference(ncpu):
+    """With wind spheres of 8 finest cells the reference algorithm goes
+    non-finite next to the strong source at the end of the dt ramp; the GPU
+    path reports WX_ERR_NAN at the same step as the CPU oracle turns
+    non-finite."""
+    from walicxe3d_b200._lib import WxError
+    prob = problems.colliding_winds(nroot=2, maxlev=3, r_wind_cells=8)
+    o = oracle.from_problem(prob, threads=ncpu)
+    g = from_problem(prob)
+    step_o = step_g = None
+    for s in range(16):
+        if step_o is None:
+            o.step()
+            if not np.isfinite(o.U[: prob.nblocks]).all():
+                step_o = s
+        if step_g is None:
+            try:
+                g.step()
+            except WxError as e:
+                assert e.code == 102
+                step_g = s
+        if step_o is not None and step_g is not None:
+            break
+    assert step_o is not None and step_o == step_g

@@ -274,22 +274,29 @@ def snr_h(nroot: int = 4, maxlev: int = 2, steps: int = 20) -> Problem:
     return _finish("snr-h", cfg, tree, prim_fn, steps)
 
 
-def colliding_winds(nroot: int = 8, maxlev: int = 6, box_pc: float = 2.0, sep_pc: float = 0.5,
-                    r_wind_pc: float = 0.05, steps: int = 500, shell_width: float = 0.25) -> Problem:
+def colliding_winds(nroot: int = 8, maxlev: int = 6, box_pc: float = 1.0, sep_pc: float = 0.5,
+                    r_wind_cells: float = 16.0, r_wind_pc: float | None = None, steps: int = 500,
+                    shell_width: float = 0.25) -> Problem:
     """Colliding stellar winds with table cooling: two spherical wind
     sources (imposeSphericalWind, winds.f90:123-240; Mdot 1e-6 and 1e-7
-    Msun/yr, vinf 2000 and 1000 km/s, T 1e5 K, radius r_wind_pc) sep_pc apart
-    on the x axis of a cubic box in a uniform n=1 cm^-3, 1e4 K ISM,
-    COOL_TABLE with a 200-row table, HLLC + minmod.  The snapshot has each
-    wind streaming freely out to the contact surface at the momentum-balance
-    stand-off distance of the weaker wind; the zone around each source is
-    refined to maxlev (as refineZone does at it=0, with a margin of one
-    finest block so no coarse/fine face meets a wind sphere's ghost layer)
-    and the bow-shaped contact region around the weaker source to
-    maxlev-1."""
+    Msun/yr, vinf 2000 and 1000 km/s, T 1e5 K, radius r_wind_cells finest
+    cells unless r_wind_pc is given) sep_pc apart on the x axis of a cubic
+    box_pc box, in a uniform n=1 cm^-3, 1e4 K ISM of neutral fraction 0.99;
+    EOS_H_RATE with the neutral-H passive scalar, COOL_TABLE with a 200-row
+    table, HLLC + minmod.  The snapshot has each wind streaming freely out
+    to the contact surface at the momentum-balance stand-off distance of the
+    weaker wind; the zone around each source is refined to maxlev (as
+    refineZone does at it=0, with a margin of one finest block so no
+    coarse/fine face meets a wind sphere's ghost layer) and the bow-shaped
+    contact region around the weaker source to maxlev-1.  The winds are
+    ionised (their passive scalar, which the reference leaves undefined, is
+    0).  With spheres of 8 finest cells or fewer the reference algorithm
+    goes non-finite next to the strong source once the dt ramp ends (the
+    stage-1 fluxes of the imposed cells use their primitives from before
+    the imposition); 16 cells run stably."""
     mu0, mu_wind = 1.3, 0.61
-    cfg = Config(npassive=0, solver_type=C.SOLVER_HLLC, limiter_type=C.LIMITER_MINMOD,
-                 eos_type=C.EOS_ADIABATIC, cooling_type=C.COOL_TABLE, nbroot=(nroot,) * 3, maxlev=maxlev,
+    cfg = Config(npassive=1, solver_type=C.SOLVER_HLLC, limiter_type=C.LIMITER_MINMOD,
+                 eos_type=C.EOS_H_RATE, cooling_type=C.COOL_TABLE, nbroot=(nroot,) * 3, maxlev=maxlev,
                  gamma=5.0 / 3.0, cfl=0.4, visc_eta=5.0e-3, l_sc=C.PC, d_sc=mu0 * C.AMU, v_sc=1.0e5,
                  box=(box_pc * C.PC,) * 3, tfin=1.0e4 * C.YR, dtout=1.0e3 * C.YR)
     L = box_pc * C.PC
@@ -297,7 +304,8 @@ def colliding_winds(nroot: int = 8, maxlev: int = 6, box_pc: float = 2.0, sep_pc
             np.array([0.5 * L + 0.5 * sep_pc * C.PC, 0.5 * L, 0.5 * L])]
     mdot = [1.0e-6 * C.MSUN / C.YR, 1.0e-7 * C.MSUN / C.YR]
     vinf = [2000.0 * C.KPS, 1000.0 * C.KPS]
-    R = r_wind_pc * C.PC
+    dx_fine = L / (NCELLS * nroot * 2 ** (maxlev - 1))
+    R = r_wind_pc * C.PC if r_wind_pc is not None else r_wind_cells * dx_fine
     winds = [[s[0], s[1], s[2], 0.0, 0.0, 0.0, R, m, v, 1.0e5, mu_wind, 0.0] for s, m, v in zip(srcs, mdot, vinf)]
     eta = (mdot[1] * vinf[1]) / (mdot[0] * vinf[0])
     r2 = sep_pc * C.PC * np.sqrt(eta) / (1.0 + np.sqrt(eta))   # stand-off of the weaker wind
@@ -324,11 +332,11 @@ def colliding_winds(nroot: int = 8, maxlev: int = 6, box_pc: float = 2.0, sep_pc
     tree.refine_where(shell, maxlev - 1)
     tree.refine_where(zone, maxlev)
 
-    def wind_prim(xyz_cm, k, prim):
+    def wind_prim(xyz_cm, k, nvar):
         d = xyz_cm - srcs[k][None, :, None, None, None]
         dist = np.maximum(np.sqrt((d ** 2).sum(axis=1)), 1.0e-3 * R)
         dens = mdot[k] / vinf[k] / dist / dist / (4.0 * C.PI)
-        out = np.zeros_like(prim)
+        out = np.zeros((xyz_cm.shape[0], nvar) + xyz_cm.shape[2:])
         out[:, 0] = dens / cfg.d_sc
         for a in range(3):
             out[:, 1 + a] = vinf[k] * d[:, a] / dist / cfg.v_sc
@@ -338,15 +346,16 @@ def colliding_winds(nroot: int = 8, maxlev: int = 6, box_pc: float = 2.0, sep_pc
     def prim_fn(xyz):
         xyz_cm = xyz * cfg.l_sc
         prim = np.zeros((xyz.shape[0], cfg.neqtot) + xyz.shape[2:])
-        n_ism, T_ism = 1.0, 1.0e4
-        prim[:, 0] = n_ism * mu0 * C.AMU / cfg.d_sc
-        prim[:, 4] = n_ism * C.KB * T_ism / cfg.p_sc
-        w1, d1 = wind_prim(xyz_cm, 0, prim)
-        w2, d2 = wind_prim(xyz_cm, 1, prim)
+        n_ism, T_ism, y_ism = 1.0, 1.0e4, 0.99
+        dens = n_ism * mu0 * C.AMU
+        prim[:, 0] = dens / cfg.d_sc
+        prim[:, 4] = dens / (mu0 * C.AMU) * C.KB * T_ism * (2.0 - y_ism) / cfg.p_sc
+        prim[:, 5] = y_ism * dens / cfg.d_sc
+        w1, d1 = wind_prim(xyz_cm, 0, cfg.neqtot)
+        w2, d2 = wind_prim(xyz_cm, 1, cfg.neqtot)
         in2 = (d2 < r2)[:, None]
         in1 = ((d1 < sep_pc * C.PC - r2) & ~(d2 < r2))[:, None]
-        prim = np.where(in2, w2, np.where(in1, w1, prim))
-        return prim
+        return np.where(in2, w2, np.where(in1, w1, prim))
 
     return _finish(f"winds-l{maxlev}", cfg, tree, prim_fn, steps, cooltable=cooling_table_synthetic(200),
                    winds=winds)
