@@ -1545,7 +1545,7 @@ extern "C" int wx3d_hydro_step_noalloc(const wx_config* cfg, int32_t nslots, con
   const int solver = cfg->solver_type;
   int zero_ghost = 0;
   auto stage = [&](void (*fn)(StageParams), size_t smem, const double* src, double* out, double factor) {
-    StageParams P{src, u_in, out, dBlocks, dWork, nwork * zsplit, zsplit, dCtl, factor, ph};
+    StageParams P{src, u_in, out, dBlocks, dWork, nwork * zsplit, zsplit, dCtl, factor, ph, 0, src};
     fn<<<noalloc_grid((const void*)fn, STAGE_THREADS, smem, nwork * zsplit, nsm), STAGE_THREADS, smem, s>>>(P);
   };
   if (solver == WX_SOLVER_LAX) {

@@ -220,8 +220,11 @@ constexpr int LIM_RUNTIME = -100;
 template <int LIM>
 __device__ __forceinline__ double average_t(double a, double b, int opt) {
   if constexpr (LIM == WX_LIMITER_MINMOD) {
-    const double s = copysign(1.0, a);
-    return s * dmax(0.0, dmin(fabs(a), s * b));
+    // s max(0, min(|a|, s b)) with s = sign(a) is the argument of smaller
+    // magnitude when a and b share a sign and (signed) zero otherwise; the
+    // product test differs only where a*b underflows (|a b| < 5e-324)
+    const double m = fabs(a) < fabs(b) ? a : b;
+    return a * b > 0.0 ? m : 0.0;
   } else if constexpr (LIM == WX_LIMITER_VANLEER) {
     const double ab = a * b;
     return (ab <= 0.0) ? 0.0 : ab * (a + b) / (a * a + b * b);

@@ -185,7 +185,7 @@ __device__ __forceinline__ void load_plane(const StageParams& P, const DevBlock&
     }
     double u[NEQ], p[NEQ], rinv;
     if (inner && c < PLANE) load_cell<NEQ>(P.src, slot, i, j, kk, u);
-    else gather_ghost<NEQ>(P.gsrc, B, slot, i, j, kk, u);
+    else gather_ghost<NEQ>(P.gsrc ? P.gsrc : P.src, B, slot, i, j, kk, u);
     const int st = flow2prim<NEQ, MHD>(u, p, ph.cv, &rinv);
     if constexpr (CH > NEQ) {
       pl[NEQ * Geo<ORDER>::PL + hidx<ORDER>(i, j)] = sqrt_nr(ph.gamma * p[4] * rinv);
