@@ -257,6 +257,19 @@ int wx3d_run_async(wx_ctx* ctx, int32_t nsteps);
  * cooling rate stored as -b (cooltable(2,i) = -b). */
 int wx3d_set_cooltable(wx_ctx* ctx, int32_t npts, const double* logT, const double* b);
 
+/* loadcooldata_metal (source/cooling.f90:193-265), COOL_TABLE_METAL: the
+ * (nptsT+1) x (nptsZ+1) table row by row as the file lists it -- first row
+ * an unused entry then the metallicities, each further row log10 T then
+ * log10 Lambda per metallicity.  The metallicity scalar is passive
+ * metalpas = 5 + 3*bfield + min(npassive, 1) (parameters.f90:318). */
+int wx3d_set_cooltable_metal(wx_ctx* ctx, int32_t nptsT, int32_t nptsZ, const double* table);
+
+/* loadcooldata_schure (source/cooling_schure.f90:52-95), COOL_SCHURE: the
+ * 180 rows of five columns of the Schure et al. table file (log10 T, then
+ * -log10 Lambda for four ionisation fractions); dmc_f (1..4) picks the
+ * column. */
+int wx3d_set_cooltable_schure(wx_ctx* ctx, const double* data, int32_t dmc_f);
+
 /* markByPhysical (source/amr.f90:142-230) for every occupied slot:
  * flags[slot] = WX_FLAG_*; empty slots get -1. */
 int wx3d_mark(wx_ctx* ctx, int32_t nslots, int32_t* flags);

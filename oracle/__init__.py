@@ -64,6 +64,8 @@ def load() -> ctypes.CDLL:
             "orc_cooling": (ctypes.c_double, [vp]),
             "orc_step": (None, [vp]),
             "orc_set_cooltable": (ctypes.c_int, [vp, ctypes.c_int, dp, dp]),
+            "orc_set_cooltable_metal": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, dp]),
+            "orc_set_cooltable_schure": (ctypes.c_int, [vp, dp, ctypes.c_int]),
             "orc_add_wind": (ctypes.c_int, [vp, dp]),
             "orc_mark": (None, [vp, ip]),
             "orc_refine": (None, [vp, ctypes.c_int, ip]),
@@ -178,6 +180,14 @@ class Oracle:
         bb = np.ascontiguousarray(b, dtype=np.float64)
         assert self.lib.orc_set_cooltable(self.h, len(lt), _dp(lt), _dp(bb)) == 0
 
+    def set_cooltable_metal(self, nptsT, nptsZ, table):
+        t = np.ascontiguousarray(table, dtype=np.float64)
+        assert self.lib.orc_set_cooltable_metal(self.h, int(nptsT), int(nptsZ), _dp(t)) == 0
+
+    def set_cooltable_schure(self, data, dmc_f):
+        d = np.ascontiguousarray(np.asarray(data).reshape(-1), dtype=np.float64)
+        assert self.lib.orc_set_cooltable_schure(self.h, _dp(d), int(dmc_f)) == 0
+
     def add_wind(self, params12):
         p = np.ascontiguousarray(params12, dtype=np.float64)
         self.lib.orc_add_wind(self.h, _dp(p))
@@ -214,6 +224,10 @@ def from_problem(prob, threads: int | None = None, extra_slots: int = 0) -> Orac
     o.set_U(prob.U)
     if prob.cooltable is not None:
         o.set_cooltable(*prob.cooltable)
+    if prob.cooltable_metal is not None:
+        o.set_cooltable_metal(*prob.cooltable_metal)
+    if prob.cooltable_schure is not None:
+        o.set_cooltable_schure(*prob.cooltable_schure)
     for w in prob.winds:
         o.add_wind(w)
     o.set_state(0.0, 0.0, 0, 1, 0)

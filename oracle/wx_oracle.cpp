@@ -70,6 +70,12 @@ struct Ctx {
   int it = 0, nextout = 1;
   bool dumpout = false;
   std::vector<double> cooltable1, cooltable2;  // cooltable(1,:), cooltable(2,:)
+  // COOL_TABLE_METAL: cooltable(nptsT+1, nptsZ+1), stored [i-1][j-1] row by row
+  std::vector<double> ctab_metal;
+  int nptsZ = 0;
+  double cool_Zmin = 0, cool_Zmax = 0;
+  // COOL_SCHURE: 180 rows of (T, Lambda), both linear
+  std::vector<double> schureT, schureL;
   int nptsT = 0;
   double cool_Tmin = 0, cool_Tmax = 0;
   std::vector<Wind> winds;
@@ -1179,7 +1185,9 @@ double find_coef(const Ctx& c, double logT) {  // cooling.f90:378-419
   return 0.0;  // NaN logT: the reference leaves coef unset
 }
 
-double apply_cooling(Ctx& c, int nb) {  // cooling.f90:285-371 (COOL_TABLE)
+double find_coef_metal(const Ctx& c, double logT, double Z);
+
+double apply_cooling(Ctx& c, int nb) {  // cooling.f90:285-371 (COOL_TABLE, COOL_TABLE_METAL)
   const double T_floor = 10.0;
   const wx_config& f = c.cfg;
   double maxloss = 0.0;
@@ -1191,11 +1199,15 @@ double apply_cooling(Ctx& c, int nb) {  // cooling.f90:285-371 (COOL_TABLE)
         for (int e = 0; e < c.neq; ++e) pv[e] = c.u(c.PRIM, nb, e)[id];
         double temp = calcTemp(c, pv);
         double logT = std::log10(temp);
+        double metal = 0.0;
+        // metalpas = neqhydro + neqmhd + min(npassive, 1) (parameters.f90:318)
+        const int metalpas = 5 + (c.cfg.bfield ? 3 : 0) + std::min(c.cfg.npassive, 1) - 1;
+        if (f.cooling_type == WX_COOL_TABLE_METAL) metal = std::fabs(pv[metalpas] / pv[0]);
         if (logT >= c.cool_Tmin) {
           double ETH = c.cv * pv[4];
           double vel2 = pv[1] * pv[1] + pv[2] * pv[2] + pv[3] * pv[3];
           double EK = 0.5 * pv[0] * vel2;
-          double aloss = find_coef(c, logT);
+          double aloss = f.cooling_type == WX_COOL_TABLE_METAL ? find_coef_metal(c, logT, metal) : find_coef(c, logT);
           double numdens = pv[0] * f.d_sc / (f.mui * AMU);
           double ce = aloss * (numdens * numdens) / (ETH * c.e_sc);
           double cool_factor = std::exp(-ce * (c.dt * c.t_sc));
@@ -1207,6 +1219,86 @@ double apply_cooling(Ctx& c, int nb) {  // cooling.f90:285-371 (COOL_TABLE)
           c.u(c.PRIM, nb, 4)[id] = pv[4] * cool_factor;
           ETH = c.cv * c.u(c.PRIM, nb, 4)[id];
           c.u(c.U, nb, 4)[id] = EK + ETH;
+        }
+      }
+  return maxloss;
+}
+
+// cooltable(i, j) of loadcooldata_metal, 1-based (cooling.f90:193-265)
+inline double ctm(const Ctx& c, int i, int j) { return c.ctab_metal[(size_t)(i - 1) * (c.nptsZ + 1) + (j - 1)]; }
+
+double find_coef_metal(const Ctx& c, double logT, double Z) {  // cooling.f90:435-519
+  if (logT < c.cool_Tmin) return 0.0;
+  int Tlo = 2, Thi = c.nptsT + 1;
+  double T0 = 0.0, T1 = 0.0;
+  if (logT <= c.cool_Tmax) {  // binary search
+    while (Thi - Tlo > 1) {
+      int Tmid = (Tlo + Thi) / 2;
+      if (logT <= ctm(c, Tmid, 1)) Thi = Tmid;
+      else Tlo = Tmid;
+    }
+    T0 = ctm(c, Tlo, 1);
+    T1 = ctm(c, Thi, 1);
+  }
+  int Zlo, Zhi;
+  if (Z < c.cool_Zmin) { Zlo = 2; Zhi = 3; }
+  else if (Z > c.cool_Zmax) { Zlo = c.nptsZ; Zhi = c.nptsZ + 1; }
+  else {
+    Zlo = 2; Zhi = c.nptsZ + 1;
+    while (Zhi - Zlo > 1) {
+      int Zmid = (Zlo + Zhi) / 2;
+      if (Z <= ctm(c, 1, Zmid)) Zhi = Zmid;
+      else Zlo = Zmid;
+    }
+  }
+  const double Z0 = ctm(c, 1, Zlo), Z1 = ctm(c, 1, Zhi);
+  if (logT >= c.cool_Tmax) {
+    // row nptsT, one below the last data row, as the reference reads it
+    const double C0 = ctm(c, c.nptsT, Zlo) + 0.5 * (logT - c.cool_Tmax);
+    const double C1 = ctm(c, c.nptsT, Zhi) + 0.5 * (logT - c.cool_Tmax);
+    return std::pow(10., (C1 - C0) / (Z1 - Z0) * (Z - Z0) + C0);
+  }
+  const double TC = (logT - T0) / (T1 - T0);
+  const double ZC = (Z - Z0) / (Z1 - Z0);
+  double coef = (1.0 - TC) * (1.0 - ZC) * ctm(c, Tlo, Zlo) + (1.0 - TC) * ZC * ctm(c, Tlo, Zhi) +
+                TC * (1.0 - ZC) * ctm(c, Thi, Zlo) + TC * ZC * ctm(c, Thi, Zhi);
+  return std::pow(10., coef);
+}
+
+double get_lambda(const Ctx& c, double T) {  // cooling_schure.f90:102-128
+  const double deltaTemp = 0.04, logTmin = 1.0;
+  if (T > 1e8) return 0.21e-26 * std::sqrt(T);
+  const int if1 = (int)((std::log10(T) - logTmin) / deltaTemp) + 1;
+  if (if1 < 1) return c.schureL[0];
+  const double T0 = c.schureT[if1 - 1], c0 = c.schureL[if1 - 1];
+  const double T1 = c.schureT[if1], c1 = c.schureL[if1];
+  return (c1 - c0) * (T - T0) / (T1 - T0) + c0;
+}
+
+double apply_cooling_schure(Ctx& c, int nb) {  // cooling_schure.f90:134-228
+  const double Tmin = 10.0;
+  const wx_config& f = c.cfg;
+  const double dt_seconds = c.dt * c.t_sc;
+  double maxloss = 0.0;
+  double pv[MAXEQ];
+  for (int i = 1; i <= NC; ++i)
+    for (int j = 1; j <= NC; ++j)
+      for (int k = 1; k <= NC; ++k) {
+        int id = cidx(i, j, k);
+        for (int e = 0; e < c.neq; ++e) pv[e] = c.u(c.PRIM, nb, e)[id];
+        double T = calcTemp(c, pv);
+        if (T > Tmin) {
+          double Lambda0 = get_lambda(c, T);
+          double gain = 0.0;
+          double dens = pv[0] / f.mu0;
+          double emtauC = std::exp(-2.0 * dt_seconds * dens * Lambda0 / (3.0 * KB * T));
+          double cool_factor = (gain / (dens * dens * Lambda0)) * (1.0 - emtauC) + emtauC;
+          double frac_loss = 1.0 - cool_factor;
+          maxloss = std::max(maxloss, frac_loss);
+          if (cool_factor < 1.0 - f.cooling_limit) cool_factor = 1.0 - f.cooling_limit;
+          c.u(c.PRIM, nb, 4)[id] = pv[4] * cool_factor;
+          const double p4 = c.u(c.PRIM, nb, 4)[id];
+          c.u(c.U, nb, 4)[id] = c.cv * p4 + 0.5 * pv[0] * (pv[1] * pv[1] + pv[2] * pv[2] + pv[3] * pv[3]);
         }
       }
   return maxloss;
@@ -1310,8 +1402,10 @@ double cooling(Ctx& c) {  // cooling.f90:37-118
   for (int nb = 0; nb < c.nbMax; ++nb) {
     if (c.localBlocks[nb] == -1) continue;
     double m = 0.0;
-    if (c.cfg.cooling_type == WX_COOL_TABLE) m = apply_cooling(c, nb);
-    else if (c.cfg.cooling_type == WX_COOL_H) m = apply_cooling_h_neq(c, nb);
+    const int ct = c.cfg.cooling_type;
+    if (ct == WX_COOL_TABLE || ct == WX_COOL_TABLE_METAL) m = apply_cooling(c, nb);
+    else if (ct == WX_COOL_SCHURE) m = apply_cooling_schure(c, nb);
+    else if (ct == WX_COOL_H) m = apply_cooling_h_neq(c, nb);
     ml = std::max(ml, m);
   }
   c.maxloss = ml;
@@ -1486,6 +1580,37 @@ void orc_step(void* h) {
   if (c->cfg.eos_type == WX_EOS_H_RATE) updateNeutralFraction(*c);
   cooling(*c);
   if (c->dumpout) { c->nextout = c->nextout + 1; c->dumpout = false; }
+}
+
+// loadcooldata_metal (cooling.f90:193-265): tab[(nptsT+1)*(nptsZ+1)] row by
+// row, tab[0][0] unused, tab[0][1..] metallicities, tab[1..][0] log T,
+// the rest log Lambda.
+int orc_set_cooltable_metal(void* h, int nptsT, int nptsZ, const double* tab) {
+  Ctx* c = static_cast<Ctx*>(h);
+  if (nptsT < 2 || nptsZ < 2) return WX_ERR_COOLING_LOAD_COEFS;
+  c->nptsT = nptsT;
+  c->nptsZ = nptsZ;
+  c->ctab_metal.assign(tab, tab + (size_t)(nptsT + 1) * (nptsZ + 1));
+  c->ctab_metal[0] = -1.0;
+  c->cool_Tmin = ctm(*c, 2, 1);
+  c->cool_Tmax = ctm(*c, nptsT + 1, 1);
+  c->cool_Zmin = ctm(*c, 1, 2);
+  c->cool_Zmax = ctm(*c, 1, nptsZ + 1);
+  return 0;
+}
+
+// loadcooldata_schure (cooling_schure.f90:52-95): 180 rows of 5 columns as
+// in the table file; column 1+dmc_f holds -log10 Lambda.
+int orc_set_cooltable_schure(void* h, const double* data, int dmc_f) {
+  Ctx* c = static_cast<Ctx*>(h);
+  if (dmc_f < 1 || dmc_f > 4) return WX_ERR_COOLING_LOAD_COEFS;
+  c->schureT.resize(180);
+  c->schureL.resize(180);
+  for (int i = 0; i < 180; ++i) {
+    c->schureT[i] = std::pow(10.0, data[5 * i]);
+    c->schureL[i] = std::pow(10.0, -data[5 * i + dmc_f]);
+  }
+  return 0;
 }
 
 int orc_set_cooltable(void* h, int npts, const double* logT, const double* b) {

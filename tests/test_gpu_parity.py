@@ -474,3 +474,20 @@ def test_small_wind_sphere_fails_at_the_same_step_as_the_reference(ncpu):
         if step_o is not None and step_g is not None:
             break
     assert step_o is not None and step_o == step_g
+
+
+@pytest.mark.parametrize("ctype", [C.COOL_TABLE, C.COOL_TABLE_METAL, C.COOL_SCHURE])
+def test_cooling_variants_match_oracle(ctype, ncpu):
+    """Tabulated cooling (cooling.f90), metallicity-dependent 2-D tables
+    (find_coef_metal, cooling.f90:435-519) and the Schure et al. tables
+    (cooling_schure.f90) on a hot dense blob, 12 main-loop iterations, and
+    the energy they remove."""
+    prob = problems.cooling_blob(ctype, nroot=2)
+    o = oracle.from_problem(prob, threads=ncpu)
+    g = from_problem(prob)
+    E0 = prob.U[:, 4].sum()
+    for _ in range(12):
+        o.step()
+        g.step()
+    check(o, g, prob)
+    assert g.download()[:, 4].sum() < (1.0 - 1e-4) * E0

@@ -48,6 +48,8 @@ _SIGNATURES = {
     "wx3d_step": (ctypes.c_int, [c_void_p, ctypes.POINTER(WxState)]),
     "wx3d_run": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.POINTER(WxState)]),
     "wx3d_run_async": (ctypes.c_int, [c_void_p, ctypes.c_int32]),
+    "wx3d_set_cooltable_metal": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.c_int32, c_double_p]),
+    "wx3d_set_cooltable_schure": (ctypes.c_int, [c_void_p, c_double_p, ctypes.c_int32]),
     "wx3d_set_cooltable": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_double_p, c_double_p]),
     "wx3d_mark": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_int32_p]),
     "wx3d_refine": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_int32_p]),

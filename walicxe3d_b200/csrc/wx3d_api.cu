@@ -159,8 +159,9 @@ struct wx_ctx {
   int32_t* dFlags = nullptr;
   DevCtl* dCtl = nullptr;
   DevCtl* hCtl = nullptr;   // pinned mirror
-  double* dCool = nullptr;  // [2][ncool]
+  double* dCool = nullptr;  // COOL_TABLE [2][ncool]; METAL [ncool+1][nZ+1]; SCHURE [2][180]
   int ncool = 0;
+  int nZ = 0;
   Tree tree;
   std::vector<int32_t> local;     // localBlocks
   std::vector<int32_t> work;      // occupied slots
@@ -229,7 +230,7 @@ int validate(const wx_config& f, std::string& why) {
     if (f.bc[i] != WX_BC_REFLECTIVE && f.bc[i] != WX_BC_FREE_FLOW) { why = "unknown boundary condition"; return WX_ERR_INVALID_ARG; }
   }
   if ((f.eos_type == WX_EOS_H_RATE || f.cooling_type == WX_COOL_H) && f.npassive < 1) { why = "H-rate EOS / COOL_H need a passive scalar"; return WX_ERR_NOT_ENOUGH_PASSIVES; }
-  if (f.cooling_type == WX_COOL_TABLE_METAL || f.cooling_type == WX_COOL_SCHURE) { why = "cooling type not supported by this ABI"; return WX_ERR_UNSUPPORTED; }
+  if (f.cooling_type < WX_COOL_NONE || f.cooling_type > WX_COOL_SCHURE) { why = "unknown cooling type"; return WX_ERR_INVALID_ARG; }
   if (f.gamma <= 1.0) { why = "gamma must exceed 1"; return WX_ERR_INVALID_ARG; }
   return WX_OK;
 }
@@ -460,7 +461,7 @@ int enqueue_sources(wx_ctx* c, int mode) {
     WX_LAUNCHED();
   }
   SrcParams P{c->dU, (mode & 4) ? c->dPrim : nullptr, c->dBlocks, c->dWork, c->nwork, mode, c->dCtl,
-              c->dCool, c->dCool ? c->dCool + c->ncool : nullptr, c->ncool, c->ph};
+              c->dCool, c->dCool ? c->dCool + c->ncool : nullptr, c->ncool, c->ph, c->nZ};
   tick(c, 3, true);
   c->k.src<<<grid_for(c, (const void*)c->k.src, 256, 0, c->nwork), 256, 0, c->stream>>>(P);
   WX_LAUNCHED();
@@ -1146,6 +1147,50 @@ int wx3d_set_cooltable(wx_ctx* c, int32_t npts, const double* logT, const double
   WX_CUDA(cudaMalloc(&c->dCool, h.size() * 8));
   WX_CUDA(cudaMemcpy(c->dCool, h.data(), h.size() * 8, cudaMemcpyHostToDevice));
   c->ncool = npts;
+  c->nZ = 0;
+  invalidate_graph(c);
+  return WX_OK;
+}
+
+// loadcooldata_metal (cooling.f90:193-265): table[(nptsT+1)*(nptsZ+1)] row
+// by row as the file lists it (first row: metallicities after an unused
+// entry; then per row log T followed by log Lambda per metallicity).
+int wx3d_set_cooltable_metal(wx_ctx* c, int32_t nptsT, int32_t nptsZ, const double* table) {
+  if (!c || !table) return WX_ERR_INVALID_ARG;
+  if (nptsT < 2 || nptsZ < 2) return fail(c, WX_ERR_COOLING_LOAD_COEFS, "metal cooling table needs 2 x 2 values");
+  const int W = nptsZ + 1;
+  std::vector<double> h(table, table + (size_t)(nptsT + 1) * W);
+  h[0] = -1.0;
+  for (int i = 2; i <= nptsT; ++i)
+    if (!(h[(size_t)i * W] > h[(size_t)(i - 1) * W])) return fail(c, WX_ERR_COOLING_LOAD_COEFS, "temperatures must increase");
+  for (int j = 2; j <= nptsZ; ++j)
+    if (!(h[j] > h[j - 1])) return fail(c, WX_ERR_COOLING_LOAD_COEFS, "metallicities must increase");
+  cudaFree(c->dCool);
+  c->dCool = nullptr;
+  WX_CUDA(cudaMalloc(&c->dCool, h.size() * 8));
+  WX_CUDA(cudaMemcpy(c->dCool, h.data(), h.size() * 8, cudaMemcpyHostToDevice));
+  c->ncool = nptsT;
+  c->nZ = nptsZ;
+  invalidate_graph(c);
+  return WX_OK;
+}
+
+// loadcooldata_schure (cooling_schure.f90:52-95): 180 rows of five columns
+// as in the table file; column 1+dmc_f (1..4) holds -log10 Lambda.
+int wx3d_set_cooltable_schure(wx_ctx* c, const double* data, int32_t dmc_f) {
+  if (!c || !data) return WX_ERR_INVALID_ARG;
+  if (dmc_f < 1 || dmc_f > 4) return fail(c, WX_ERR_COOLING_LOAD_COEFS, "dmc_f selects column 2..5 (1..4)");
+  std::vector<double> h(360);
+  for (int i = 0; i < 180; ++i) {
+    h[i] = std::pow(10.0, data[5 * i]);
+    h[180 + i] = std::pow(10.0, -data[5 * i + dmc_f]);
+  }
+  cudaFree(c->dCool);
+  c->dCool = nullptr;
+  WX_CUDA(cudaMalloc(&c->dCool, h.size() * 8));
+  WX_CUDA(cudaMemcpy(c->dCool, h.data(), h.size() * 8, cudaMemcpyHostToDevice));
+  c->ncool = 180;
+  c->nZ = 0;
   invalidate_graph(c);
   return WX_OK;
 }

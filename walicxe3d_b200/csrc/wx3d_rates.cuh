@@ -112,6 +112,60 @@ __device__ __forceinline__ double find_coef(const double* __restrict__ lt, const
   return pow(10., (C1 - C0) / (T1 - T0) * (logT - T0) + C0);
 }
 
+// find_coef_metal (cooling.f90:435-519) on cooltable(nT+1, nZ+1) stored row
+// by row: row 0 holds the metallicities, column 0 the log temperatures.
+// Above the last temperature the reference extrapolates from row nptsT, one
+// below the last data row; that row is used here as well.
+__device__ __forceinline__ double find_coef_metal(const double* __restrict__ tab, int nT, int nZ, double logT,
+                                                  double Z) {
+  const int W = nZ + 1;
+  auto ct = [&](int i, int j) { return tab[(i - 1) * W + (j - 1)]; };  // 1-based as the reference
+  const double Tmin = ct(2, 1), Tmax = ct(nT + 1, 1);
+  if (logT < Tmin) return 0.0;
+  int Tlo = 2, Thi = nT + 1;
+  double T0 = 0.0, T1 = 0.0;
+  if (logT <= Tmax) {
+    while (Thi - Tlo > 1) {
+      const int Tmid = (Tlo + Thi) / 2;
+      if (logT <= ct(Tmid, 1)) Thi = Tmid; else Tlo = Tmid;
+    }
+    T0 = ct(Tlo, 1);
+    T1 = ct(Thi, 1);
+  }
+  int Zlo, Zhi;
+  if (Z < ct(1, 2)) { Zlo = 2; Zhi = 3; }
+  else if (Z > ct(1, nZ + 1)) { Zlo = nZ; Zhi = nZ + 1; }
+  else {
+    Zlo = 2; Zhi = nZ + 1;
+    while (Zhi - Zlo > 1) {
+      const int Zmid = (Zlo + Zhi) / 2;
+      if (Z <= ct(1, Zmid)) Zhi = Zmid; else Zlo = Zmid;
+    }
+  }
+  const double Z0 = ct(1, Zlo), Z1 = ct(1, Zhi);
+  if (logT >= Tmax) {
+    const double C0 = ct(nT, Zlo) + 0.5 * (logT - Tmax);
+    const double C1 = ct(nT, Zhi) + 0.5 * (logT - Tmax);
+    return pow(10., (C1 - C0) / (Z1 - Z0) * (Z - Z0) + C0);
+  }
+  const double TC = (logT - T0) / (T1 - T0);
+  const double ZC = (Z - Z0) / (Z1 - Z0);
+  const double coef = (1.0 - TC) * (1.0 - ZC) * ct(Tlo, Zlo) + (1.0 - TC) * ZC * ct(Tlo, Zhi) +
+                      TC * (1.0 - ZC) * ct(Thi, Zlo) + TC * ZC * ct(Thi, Zhi);
+  return pow(10., coef);
+}
+
+// get_lambda (cooling_schure.f90:102-128): 180 rows of linear T and Lambda,
+// rows 0.04 dex apart from log T = 1.
+__device__ __forceinline__ double get_lambda_schure(const double* __restrict__ Tt, const double* __restrict__ Lt,
+                                                    double T) {
+  if (T > 1e8) return 0.21e-26 * sqrt(T);
+  const int if1 = (int)((log10(T) - 1.0) / 0.04) + 1;
+  if (if1 < 1) return Lt[0];
+  const double T0 = Tt[if1 - 1], c0 = Lt[if1 - 1], T1 = Tt[if1], c1 = Lt[if1];
+  return (c1 - c0) * (T - T0) / (T1 - T0) + c0;
+}
+
 // One plain step of updateNeutralFraction then apply_cooling_h_neq for a cell
 // (hrate.f90:101-140, cooling_h.f90:175-246) on its conserved u and
 // primitive p vectors -- the arithmetic of source_kernel's fused H_RATE +

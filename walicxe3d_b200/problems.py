@@ -31,6 +31,8 @@ class Problem:
     local_blocks: np.ndarray      # int32 bID per slot
     U: np.ndarray                 # float64 [nslots, neq, 16, 16, 16]
     cooltable: tuple | None = None
+    cooltable_metal: tuple | None = None    # (nptsT, nptsZ, table[(nptsT+1)*(nptsZ+1)])
+    cooltable_schure: tuple | None = None   # (data[180, 5], dmc_f)
     winds: list = field(default_factory=list)
     steps: int = 50
 
@@ -359,3 +361,71 @@ def colliding_winds(nroot: int = 8, maxlev: int = 6, box_pc: float = 1.0, sep_pc
 
     return _finish(f"winds-l{maxlev}", cfg, tree, prim_fn, steps, cooltable=cooling_table_synthetic(200),
                    winds=winds)
+
+
+def metal_table_synthetic(nT: int = 60, Z=(0.1, 0.3, 1.0, 3.0)) -> tuple:
+    """A COOL_TABLE_METAL table in loadcooldata_metal layout
+    (source/cooling.f90:193-265): log T from 4 to 8.5, log Lambda rising
+    with log Z and peaking near 1e5.3 K."""
+    logT = np.linspace(4.0, 8.5, nT)
+    tab = np.zeros((nT + 1, len(Z) + 1))
+    tab[0, 0] = -1.0
+    tab[0, 1:] = Z
+    tab[1:, 0] = logT
+    base = -21.8 - 0.8 * (logT - 5.3) ** 2 / (1.0 + 0.4 * np.abs(logT - 5.3))
+    for j, z in enumerate(Z):
+        tab[1:, j + 1] = base + 0.6 * np.log10(z) * np.exp(-0.5 * (logT - 5.5) ** 2)
+    return nT, len(Z), tab.ravel()
+
+
+def schure_table_synthetic() -> np.ndarray:
+    """A Schure et al. style table (source/cooling_schure.f90:52-95): 180
+    rows of log T (1.0 to 8.16 by 0.04) and -log Lambda for four ionisation
+    fractions of the low-temperature branch."""
+    logT = 1.0 + 0.04 * np.arange(180)
+    data = np.zeros((180, 5))
+    data[:, 0] = logT
+    hot = 21.7 + 0.8 * (logT - 5.3) ** 2 / (1.0 + 0.4 * np.abs(logT - 5.3))
+    for c, fi in enumerate((1e-4, 1e-3, 1e-2, 1e-1)):
+        cold = 26.0 - 0.5 * np.log10(fi) - 0.6 * (logT - 4.0)
+        w = 0.5 * (1.0 + np.tanh((logT - 4.2) / 0.15))
+        data[:, 1 + c] = w * hot + (1.0 - w) * np.minimum(cold, 29.0)
+    return data
+
+
+def cooling_blob(cooling_type: int, nroot: int = 4, steps: int = 10) -> Problem:
+    """A hot, dense blob in a warm medium, in physical units (box 1 pc,
+    l_sc = pc, d_sc = 1.3 amu, v_sc = 1 km/s): n from 10 to 1000 cm^-3 and T
+    from 1e4 to 3e7 K, smooth, with a metallicity passive scalar of 0.05 to
+    4 times the density (COOL_TABLE_METAL reads it), slow expansion.  For
+    COOL_TABLE, COOL_TABLE_METAL and COOL_SCHURE with synthetic tables;
+    cooling removes percents of the thermal energy per step."""
+    mu0 = 1.3
+    cfg = Config(npassive=1, solver_type=C.SOLVER_HLLC, limiter_type=C.LIMITER_MINMOD,
+                 eos_type=C.EOS_SINGLE_SPECIE, cooling_type=cooling_type, nbroot=(nroot,) * 3, maxlev=1,
+                 gamma=5.0 / 3.0, cfl=0.4, visc_eta=5.0e-3, l_sc=C.PC, d_sc=mu0 * C.AMU, v_sc=1.0e5,
+                 box=(C.PC,) * 3, tfin=1.0e9 * C.YR, dtout=1.0e9 * C.YR)
+    tree = BlockTree(cfg.nbroot, 1).roots()
+    c = np.array([0.5, 0.5, 0.5])
+
+    def prim_fn(xyz):
+        r = np.sqrt(((xyz - c[None, :, None, None, None]) ** 2).sum(axis=1))
+        prim = np.zeros((xyz.shape[0], cfg.neqtot) + xyz.shape[2:])
+        n = 10.0 + 990.0 * np.exp(-(r / 0.15) ** 2)
+        T = 1.0e4 + 3.0e7 * np.exp(-(r / 0.12) ** 2)
+        prim[:, 0] = n
+        prim[:, 4] = n * mu0 * C.AMU / (mu0 * C.AMU) * C.KB * T / cfg.p_sc
+        rr = np.maximum(r, 1e-12)
+        for d in range(3):
+            prim[:, 1 + d] = 3.0 * r * (xyz[:, d] - c[d]) / rr
+        prim[:, 5] = n * (0.05 + 3.95 * 0.5 * (1.0 + np.sin(12.0 * xyz[:, 0]) * np.cos(9.0 * xyz[:, 1])))
+        return prim
+
+    kw = {}
+    if cooling_type == C.COOL_TABLE:
+        kw["cooltable"] = cooling_table_synthetic(200)
+    elif cooling_type == C.COOL_TABLE_METAL:
+        kw["cooltable_metal"] = metal_table_synthetic()
+    elif cooling_type == C.COOL_SCHURE:
+        kw["cooltable_schure"] = (schure_table_synthetic(), 2)
+    return _finish(f"cooling-blob-{cooling_type}", cfg, tree, prim_fn, steps, **kw)

@@ -186,6 +186,14 @@ class Walicxe3D:
         self._chk(self.lib.wx3d_cooling(self.ctx, ctypes.byref(m)), "wx3d_cooling")
         return m.value
 
+    def set_cooltable_metal(self, nptsT, nptsZ, table):
+        t, p = _f64(table)
+        self._chk(self.lib.wx3d_set_cooltable_metal(self.ctx, int(nptsT), int(nptsZ), p), "wx3d_set_cooltable_metal")
+
+    def set_cooltable_schure(self, data, dmc_f):
+        d, p = _f64(np.asarray(data).reshape(-1))
+        self._chk(self.lib.wx3d_set_cooltable_schure(self.ctx, p, int(dmc_f)), "wx3d_set_cooltable_schure")
+
     def sources(self) -> float:
         """updatePrims + updateNeutralFraction + cooling in one fused pass
         (the surrogate's, when attached); returns maxloss."""
@@ -266,6 +274,10 @@ def from_problem(prob, extra_slots: int = 0) -> Walicxe3D:
     w.upload(prob.U)
     if prob.cooltable is not None:
         w.set_cooltable(*prob.cooltable)
+    if prob.cooltable_metal is not None:
+        w.set_cooltable_metal(*prob.cooltable_metal)
+    if prob.cooltable_schure is not None:
+        w.set_cooltable_schure(*prob.cooltable_schure)
     if prob.winds:
         w.set_winds(prob.winds)
     w.set_state(time=0.0, dt=0.0, it=0, nextout=1)
