@@ -77,6 +77,9 @@ enum {
   WX_ERR_INSUFICIENT_NBMAXPROC = 7,
   WX_ERR_TOO_MANY_LEVS = 12,
   WX_ERR_COOLING_LOAD_COEFS = 14,
+  WX_ERR_OUTPUT_FILE_OPEN = 18,
+  WX_ERR_WARM_FILE_OPEN = 20,
+  WX_ERR_WARM_READ_BLOCKS = 21,
   WX_ERR_DIVISION_BY_ZERO = 23,
   WX_ERR_NOT_ENOUGH_PASSIVES = 26,
   WX_ERR_NAN_IN_FLUXES = 27,
@@ -201,6 +204,22 @@ int wx3d_set_fusion(wx_ctx* ctx, int32_t fuse_viscous);
  * order, best (may be NULL) two values: the chosen split and the fusion
  * flag. */
 int wx3d_autotune(wx_ctx* ctx, int32_t reps, double* ms5, int32_t* best);
+
+/* Checkpoints in the reference's formats, written from and read into HBM.
+ * wx3d_write_bin: writeBin (source/output.f90:156-213), a stream file of
+ * int32 nbLocal then, per occupied slot in slot order, int32 bID and
+ * U(nb,:,1:16,1:16,1:16) in FP64 with the equation index fastest.
+ * wx3d_read_bin: warmstart's block read (source/init.f90:589-612): blocks go
+ * to slots 0..nbLocal-1 in file order, the neighbour table is rebuilt, and
+ * local_blocks[max_slots] receives the registry (-1 beyond nbLocal).
+ * wx3d_write_state / wx3d_read_state: writeState (output.f90:219-263) and
+ * warmstart's state read (init.f90:549-573), '(es22.15,i8,i5)' with
+ * time*t_sc, it, noutput, then the data directory; reading sets time, it
+ * and nextout = noutput + 1. */
+int wx3d_write_bin(wx_ctx* ctx, const char* path);
+int wx3d_read_bin(wx_ctx* ctx, const char* path, int32_t max_slots, int32_t* local_blocks, int32_t* nblocks);
+int wx3d_write_state(wx_ctx* ctx, const char* path, int32_t noutput, const char* datadir);
+int wx3d_read_state(wx_ctx* ctx, const char* path, int32_t* noutput, char* datadir, int32_t nbytes);
 
 /* Conserved variables, native layout: u[slot][eq][k][j][i], 16^3 physical
  * cells per block, host memory (pinned or pageable). */

@@ -33,6 +33,10 @@ _SIGNATURES = {
     "wx3d_set_winds": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_double_p]),
     "wx3d_autotune": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_double_p, c_int32_p]),
     "wx3d_get_neighbours": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_int32_p, c_int32_p]),
+    "wx3d_write_bin": (ctypes.c_int, [c_void_p, ctypes.c_char_p]),
+    "wx3d_read_bin": (ctypes.c_int, [c_void_p, ctypes.c_char_p, ctypes.c_int32, c_int32_p, c_int32_p]),
+    "wx3d_write_state": (ctypes.c_int, [c_void_p, ctypes.c_char_p, ctypes.c_int32, ctypes.c_char_p]),
+    "wx3d_read_state": (ctypes.c_int, [c_void_p, ctypes.c_char_p, c_int32_p, ctypes.c_char_p, ctypes.c_int32]),
     "wx3d_upload_blocks": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_double_p]),
     "wx3d_download_blocks": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_double_p]),
     "wx3d_upload_U_fortran": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_double_p]),

@@ -581,6 +581,9 @@ const char* wx3d_error_string(int32_t code) {
     case WX_ERR_INSUFICIENT_NBMAXPROC: return "not enough block slots";
     case WX_ERR_TOO_MANY_LEVS: return "too many refinement levels";
     case WX_ERR_COOLING_LOAD_COEFS: return "bad cooling table";
+    case WX_ERR_OUTPUT_FILE_OPEN: return "could not write an output file";
+    case WX_ERR_WARM_FILE_OPEN: return "could not read a warm-start file";
+    case WX_ERR_WARM_READ_BLOCKS: return "warm-start block file is short or malformed";
     case WX_ERR_DIVISION_BY_ZERO: return "zero density";
     case WX_ERR_NOT_ENOUGH_PASSIVES: return "not enough passive scalars";
     case WX_ERR_NAN_IN_FLUXES: return "NaN in fluxes";
@@ -905,6 +908,154 @@ static int ensure_stage(wx_ctx* c, size_t bytes) {
   c->stage_bytes = 0;
   WX_CUDA(cudaMalloc(&c->dStage, bytes));
   c->stage_bytes = bytes;
+  return WX_OK;
+}
+
+// ---- checkpoints: writeBin / writeState / warmstart --------------------------
+
+// writeBin (output.f90:156-213): stream file of int32 nbLocal, then per
+// occupied slot in slot order int32 bID and U(nb,:,1:16,1:16,1:16) (FP64,
+// equation index fastest), written from device memory in chunks.
+int wx3d_write_bin(wx_ctx* c, const char* path) {
+  if (!c || !path) return WX_ERR_INVALID_ARG;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(c, WX_ERR_OUTPUT_FILE_OPEN, "could not open %s", path);
+  const int32_t nloc = c->nwork;
+  int rc = WX_OK;
+  const int chunk = 256;
+  const size_t per = (size_t)c->neq * BCELLS;
+  double* host = nullptr;
+  int32_t* dslots = nullptr;
+  if (std::fwrite(&nloc, 4, 1, f) != 1) rc = fail(c, WX_ERR_OUTPUT_FILE_OPEN, "write failed: %s", path);
+  if (!rc) rc = ensure_stage(c, chunk * per * 8);
+  if (!rc && (cudaMallocHost(&host, chunk * per * 8) != cudaSuccess || cudaMalloc(&dslots, 4 * chunk) != cudaSuccess))
+    rc = fail(c, WX_ERR_CUDA, "checkpoint buffers");
+  for (int b0 = 0; !rc && b0 < nloc; b0 += chunk) {
+    const int nb = std::min(chunk, nloc - b0);
+    cudaMemcpyAsync(dslots, c->work.data() + b0, 4 * nb, cudaMemcpyHostToDevice, c->stream);
+    pack_bin_kernel<<<1184, 256, 0, c->stream>>>(c->dU, dslots, nb, c->neq, c->dStage);
+    cudaMemcpyAsync(host, c->dStage, nb * per * 8, cudaMemcpyDeviceToHost, c->stream);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) { rc = fail(c, WX_ERR_CUDA, "checkpoint copy"); break; }
+    for (int b = 0; b < nb; ++b) {
+      const int32_t bid = c->local[c->work[b0 + b]];
+      if (std::fwrite(&bid, 4, 1, f) != 1 || std::fwrite(host + b * per, 8, per, f) != per) {
+        rc = fail(c, WX_ERR_OUTPUT_FILE_OPEN, "write failed: %s", path);
+        break;
+      }
+    }
+  }
+  if (std::fclose(f) != 0 && !rc) rc = fail(c, WX_ERR_OUTPUT_FILE_OPEN, "close failed: %s", path);
+  cudaFreeHost(host);
+  cudaFree(dslots);
+  return rc;
+}
+
+// warmstart's block read (init.f90:589-612): the file's blocks go to slots
+// 0..nbLocal-1 in file order (localBlocks(nb) = bID), the neighbour table is
+// rebuilt for them, and local_blocks (max_slots entries, -1 beyond nbLocal)
+// receives the registry for the host's block tree.
+int wx3d_read_bin(wx_ctx* c, const char* path, int32_t max_slots, int32_t* local_blocks, int32_t* nblocks) {
+  if (!c || !path || !local_blocks || max_slots <= 0) return WX_ERR_INVALID_ARG;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(c, WX_ERR_WARM_FILE_OPEN, "could not open %s", path);
+  int32_t nloc = 0;
+  if (std::fread(&nloc, 4, 1, f) != 1 || nloc < 0) { std::fclose(f); return fail(c, WX_ERR_WARM_READ_BLOCKS, "bad header in %s", path); }
+  if (nloc > c->max_blocks || nloc > max_slots) {
+    std::fclose(f);
+    return fail(c, WX_ERR_INSUFICIENT_NBMAXPROC, "%d blocks in %s exceed the %d slots", nloc, path, std::min(c->max_blocks, max_slots));
+  }
+  const size_t per = (size_t)c->neq * BCELLS;
+  const int chunk = 256;
+  int rc = ensure_stage(c, chunk * per * 8);
+  double* host = nullptr;
+  if (!rc && cudaMallocHost(&host, chunk * per * 8) != cudaSuccess) rc = fail(c, WX_ERR_CUDA, "checkpoint buffers");
+  std::vector<int32_t> lb(max_slots, -1);
+  for (int b0 = 0; !rc && b0 < nloc; b0 += chunk) {
+    const int nb = std::min(chunk, nloc - b0);
+    for (int b = 0; b < nb; ++b) {
+      if (std::fread(&lb[b0 + b], 4, 1, f) != 1 || std::fread(host + b * per, 8, per, f) != per) {
+        rc = fail(c, WX_ERR_WARM_READ_BLOCKS, "read %d of %d blocks from %s", b0 + b, nloc, path);
+        break;
+      }
+    }
+    if (rc) break;
+    cudaMemcpyAsync(c->dStage, host, nb * per * 8, cudaMemcpyHostToDevice, c->stream);
+    unpack_bin_kernel<<<1184, 256, 0, c->stream>>>(c->dStage, b0, nb, c->neq, c->dU);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) rc = fail(c, WX_ERR_CUDA, "checkpoint copy");
+  }
+  std::fclose(f);
+  cudaFreeHost(host);
+  if (rc) return rc;
+  if ((rc = wx3d_set_mesh(c, std::min(max_slots, c->max_blocks), lb.data()))) return rc;
+  std::copy(lb.begin(), lb.end(), local_blocks);
+  if (nblocks) *nblocks = nloc;
+  c->dt_valid = false;
+  c->prestep = false;
+  return WX_OK;
+}
+
+// Fortran ES22.15 of x: the exponent letter is dropped when three exponent
+// digits are needed.
+static void fortran_es22_15(double x, char* out) {
+  char buf[64];
+  std::snprintf(buf, sizeof buf, "%.15E", x);
+  char* e = std::strchr(buf, 'E');
+  if (e) {
+    const int ex = std::atoi(e + 1);
+    if (ex >= 100 || ex <= -100) std::snprintf(e, sizeof buf - (e - buf), "%+04d", ex);
+  }
+  std::snprintf(out, 32, "%22s", buf);
+}
+
+// writeState (output.f90:219-263): '(es22.15,i8,i5)' time*t_sc, it, noutput,
+// then the data directory.
+int wx3d_write_state(wx_ctx* c, const char* path, int32_t noutput, const char* datadir) {
+  if (!c || !path) return WX_ERR_INVALID_ARG;
+  WX_CUDA(cudaMemcpyAsync(c->hCtl, c->dCtl, sizeof(DevCtl), cudaMemcpyDeviceToHost, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  FILE* f = std::fopen(path, "w");
+  if (!f) return fail(c, WX_ERR_OUTPUT_FILE_OPEN, "could not open %s", path);
+  char t[32];
+  fortran_es22_15(c->hCtl->time * c->ph.t_sc, t);
+  std::fprintf(f, "%s%8d%5d\n%s\n", t, c->hCtl->it, noutput, datadir ? datadir : "");
+  return std::fclose(f) == 0 ? WX_OK : fail(c, WX_ERR_OUTPUT_FILE_OPEN, "close failed: %s", path);
+}
+
+// warmstart's state read (init.f90:549-573): time (cgs), it and noutput;
+// the context takes time/t_sc, it and nextout = noutput + 1.  datadir
+// (nbytes, may be NULL) receives the second line.
+int wx3d_read_state(wx_ctx* c, const char* path, int32_t* noutput, char* datadir, int32_t nbytes) {
+  if (!c || !path) return WX_ERR_INVALID_ARG;
+  FILE* f = std::fopen(path, "r");
+  if (!f) return fail(c, WX_ERR_WARM_FILE_OPEN, "could not open %s", path);
+  char line[512] = {0}, dir[512] = {0};
+  const bool ok = std::fgets(line, sizeof line, f) != nullptr;
+  if (std::fgets(dir, sizeof dir, f)) dir[std::strcspn(dir, "\r\n")] = 0;
+  std::fclose(f);
+  if (!ok || std::strlen(line) < 35) return fail(c, WX_ERR_WARM_FILE_OPEN, "bad state line in %s", path);
+  // fixed columns: 22 for the time, 8 for it, 5 for noutput
+  char tt[23] = {0}, ti[9] = {0}, tn[6] = {0};
+  std::memcpy(tt, line, 22);
+  std::memcpy(ti, line + 22, 8);
+  std::memcpy(tn, line + 30, 5);
+  // a three-digit exponent without its letter: put the E back
+  std::string ts(tt);
+  const size_t pos = ts.find_last_of("+-");
+  if (ts.find_first_of("Ee") == std::string::npos && pos != std::string::npos && pos > ts.find_first_not_of(' ') + 1)
+    ts.insert(pos, "E");
+  wx_state st{};
+  st.time = std::strtod(ts.c_str(), nullptr) / c->ph.t_sc;
+  st.it = std::atoi(ti);
+  const int nout = std::atoi(tn);
+  st.nextout = nout + 1;
+  st.dt = 0.0;
+  int rc = wx3d_set_state(c, &st);
+  if (rc) return rc;
+  if (noutput) *noutput = nout;
+  if (datadir && nbytes > 0) {
+    std::strncpy(datadir, dir, nbytes - 1);
+    datadir[nbytes - 1] = 0;
+  }
   return WX_OK;
 }
 

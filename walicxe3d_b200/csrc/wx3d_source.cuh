@@ -320,4 +320,29 @@ __global__ void native_to_fortran(const double* __restrict__ u, double* __restri
   }
 }
 
+// writeBin / warmstart (output.f90:156-213, init.f90:527-623) store each
+// block as U(nb, :, 1:16, 1:16, 1:16): the equation index fastest, then i,
+// j, k.  pack: slots slot0.. of the native state -> nb consecutive blocks
+// of that order; unpack: the reverse.
+__global__ void pack_bin_kernel(const double* __restrict__ u, const int32_t* __restrict__ slots, int nb, int neq,
+                                double* __restrict__ out) {
+  const long long n = (long long)nb * BCELLS * neq;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(q % neq);
+    const long long cell = q / neq;           // block-major, then k, j, i (i fastest)
+    const int b = (int)(cell / BCELLS), c = (int)(cell % BCELLS);
+    out[q] = u[((size_t)slots[b] * neq + e) * BCELLS + c];
+  }
+}
+
+__global__ void unpack_bin_kernel(const double* __restrict__ in, int slot0, int nb, int neq, double* __restrict__ u) {
+  const long long n = (long long)nb * BCELLS * neq;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(q % neq);
+    const long long cell = q / neq;
+    const int b = (int)(cell / BCELLS), c = (int)(cell % BCELLS);
+    u[((size_t)(slot0 + b) * neq + e) * BCELLS + c] = in[q];
+  }
+}
+
 }  // namespace wx

@@ -186,6 +186,32 @@ class Walicxe3D:
         self._chk(self.lib.wx3d_cooling(self.ctx, ctypes.byref(m)), "wx3d_cooling")
         return m.value
 
+    # -- checkpoints (writeBin / writeState / warmstart) ----------------------
+    def write_bin(self, path):
+        self._chk(self.lib.wx3d_write_bin(self.ctx, str(path).encode()), "wx3d_write_bin")
+
+    def read_bin(self, path) -> np.ndarray:
+        """warmstart's block read: returns the new localBlocks registry."""
+        lb = np.full(self.max_blocks, -1, np.int32)
+        n = ctypes.c_int32()
+        self._chk(self.lib.wx3d_read_bin(self.ctx, str(path).encode(), self.max_blocks,
+                                         lb.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(n)),
+                  "wx3d_read_bin")
+        self.nslots = int(n.value)
+        return lb
+
+    def write_state(self, path, noutput: int, datadir: str = ""):
+        self._chk(self.lib.wx3d_write_state(self.ctx, str(path).encode(), int(noutput), datadir.encode()),
+                  "wx3d_write_state")
+
+    def read_state(self, path):
+        """warmstart's state read; returns (noutput, datadir)."""
+        n = ctypes.c_int32()
+        buf = ctypes.create_string_buffer(512)
+        self._chk(self.lib.wx3d_read_state(self.ctx, str(path).encode(), ctypes.byref(n), buf, 512),
+                  "wx3d_read_state")
+        return int(n.value), buf.value.decode()
+
     def set_cooltable_metal(self, nptsT, nptsZ, table):
         t, p = _f64(table)
         self._chk(self.lib.wx3d_set_cooltable_metal(self.ctx, int(nptsT), int(nptsZ), p), "wx3d_set_cooltable_metal")
