@@ -304,8 +304,10 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
       }
       if (t < 17 * NC) {
         const double* pp = ring + ring_slot(m) * CH * Geo<ORDER>::PL;
-        {  // x-interface between ii and ii+1 in row jx
-          const int ii = t % 17, jx = t / 17 + 1;
+        {  // x-interface between ii and ii+1 in row jx: a half-warp takes 16
+           // consecutive interfaces of one row (conflict-free shared loads),
+           // threads 256..271 the last interface of each row
+          const int ii = t < PLANE ? (t & 15) : NC, jx = t < PLANE ? (t >> 4) + 1 : t - PLANE + 1;
           double f[NEQ];
           iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 0>(pp + hidx<ORDER>(ii - 1, jx), pp + hidx<ORDER>(ii, jx), pp + hidx<ORDER>(ii + 1, jx),
                                                  pp + hidx<ORDER>(ii + 2, jx), ph, f);
