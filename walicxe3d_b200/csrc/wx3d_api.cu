@@ -996,7 +996,7 @@ int wx3d_read_bin(wx_ctx* c, const char* path, int32_t max_slots, int32_t* local
 
 // Fortran ES22.15 of x: the exponent letter is dropped when three exponent
 // digits are needed.
-static void fortran_es22_15(double x, char* out) {
+static void fortran_es22_15(double x, char* out) {   // out: at least 64 bytes
   char buf[64];
   std::snprintf(buf, sizeof buf, "%.15E", x);
   char* e = std::strchr(buf, 'E');
@@ -1004,7 +1004,9 @@ static void fortran_es22_15(double x, char* out) {
     const int ex = std::atoi(e + 1);
     if (ex >= 100 || ex <= -100) std::snprintf(e, sizeof buf - (e - buf), "%+04d", ex);
   }
-  std::snprintf(out, 32, "%22s", buf);
+  const size_t n = std::strlen(buf);
+  std::memset(out, ' ', 22 > n ? 22 - n : 0);
+  std::memcpy(out + (22 > n ? 22 - n : 0), buf, n + 1);
 }
 
 // writeState (output.f90:219-263): '(es22.15,i8,i5)' time*t_sc, it, noutput,
@@ -1015,7 +1017,7 @@ int wx3d_write_state(wx_ctx* c, const char* path, int32_t noutput, const char* d
   WX_CUDA(cudaStreamSynchronize(c->stream));
   FILE* f = std::fopen(path, "w");
   if (!f) return fail(c, WX_ERR_OUTPUT_FILE_OPEN, "could not open %s", path);
-  char t[32];
+  char t[64];
   fortran_es22_15(c->hCtl->time * c->ph.t_sc, t);
   std::fprintf(f, "%s%8d%5d\n%s\n", t, c->hCtl->it, noutput, datadir ? datadir : "");
   return std::fclose(f) == 0 ? WX_OK : fail(c, WX_ERR_OUTPUT_FILE_OPEN, "close failed: %s", path);
@@ -1712,7 +1714,6 @@ extern "C" int wx3d_hydro_step_noalloc(const wx_config* cfg, int32_t nslots, con
   }
   if (nwork == 0) return WX_ERR_MESH;
   int zsplit = 1;
-  bool fuse = true;   // corrector carries the viscous step when zsplit == 1
   while (zsplit < 8 && nwork * zsplit < 2 * nsm) zsplit *= 2;
 
   PhysParams ph{};
