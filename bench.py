@@ -197,6 +197,60 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_partition(args, prob, rank, world, dist):
+    """One mesh shared by the ranks (walicxe3d_b200.partition): each owns a
+    Morton share plus halo copies, exchanged over NCCL between the stages;
+    timed with CUDA events on the library stream, max over ranks."""
+    import torch
+    from walicxe3d_b200.partition import Rank, TorchDist, make_plan
+    plans = make_plan(prob.local_blocks, prob.cfg.nbroot, prob.cfg.maxlev, world)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    r = Rank(prob, plans[rank], stream.cuda_stream)
+    if dist is None:
+        class _Local:   # one rank: the parts without exchanges
+            def __init__(self, r):
+                self.r = r
+
+            def step(self):
+                self.r.set_dtmin(self.r.dtmin())
+                for p in range(4):
+                    self.r.part(p)
+        tr = _Local(r)
+    else:
+        tr = TorchDist(r)
+    for _ in range(args.warmup):
+        tr.step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        tr.step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    if rank == 0:
+        line = {"metric": "Mcell-updates/s", "value": prob.cells * args.steps / (ms / 1e3) / 1e6,
+                "unit": "Mcell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": args.workload, "description": WORKLOADS[args.workload]["desc"],
+                           "blocks": prob.nblocks, "cells": prob.cells,
+                           "parallelism": f"block partition x{world} (Morton shares, halo blocks over NCCL)",
+                           "halo_blocks": [len(p.halo) for p in plans]}}
+        print(json.dumps(line), flush=True)
+    r.w.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -206,6 +260,8 @@ def main():
     ap.add_argument("--workload", default="blast-amr", choices=sorted(WORKLOADS))
     ap.add_argument("--zsplit", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--partition", action="store_true",
+                    help="strong scaling: the ranks share one mesh (halo exchange over NCCL) instead of replicas")
     ap.add_argument("--surrogate", action="store_true",
                     help="attach the trained hrate + cooling_h surrogate (EOS_H_RATE + COOL_H workloads)")
     args = ap.parse_args()
@@ -233,6 +289,8 @@ def main():
     from walicxe3d_b200.solver import from_problem
 
     prob = build_problem(args.workload)
+    if args.partition:
+        return run_partition(args, prob, rank, world, dist)
     w = from_problem(prob)
     # a dedicated stream: the library runs on it and the timing events are
     # recorded on it (the default stream's handle 0 would select the

@@ -164,6 +164,16 @@ int wx3d_set_stream(wx_ctx* ctx, void* cuda_stream);
  * neighbour table with the reference's tree queries (source/amr.f90:439-631). */
 int wx3d_set_mesh(wx_ctx* ctx, int32_t nslots, const int32_t* local_blocks);
 
+/* A process's share of a partitioned mesh: as wx3d_set_mesh, with nhalo of
+ * the slots (halo_slots) holding copies of blocks other processes own --
+ * read as neighbours by the stages, never updated, their own faces allowed
+ * to lead out of the local set.  The host refreshes them with
+ * wx3d_pack_blocks/wx3d_unpack_blocks before each stage (the MPI halo
+ * exchange of boundary.f90:174-291 and :357-555).  Wind sources are not
+ * supported in this mode. */
+int wx3d_set_mesh_halo(wx_ctx* ctx, int32_t nslots, const int32_t* local_blocks, int32_t nhalo,
+                       const int32_t* halo_slots);
+
 /* Device neighbour table as built by wx3d_set_mesh, for inspection:
  * per slot and face (6): type, 4 neighbour slots.  face_type[nslots*6],
  * face_slot[nslots*24]; empty slots report type 0. */
@@ -380,6 +390,28 @@ int wx3d_check_fast_math(int32_t n, const double* host_x, int64_t* max_ulp2);
 /* Measured FP64 FMA throughput of the current device in GFLOP/s (an FMA
  * counts two flops): the compute roofline of the stage kernels. */
 int wx3d_measure_fp64_peak(double* gflops);
+
+/* The main-loop iteration in parts, for partitioned runs that exchange
+ * halo blocks between the stages:
+ *   part 0: getTimestep's tail (dt from the CFL minimum, it += 1);
+ *   part 1: the first stage (predictor, or the single stage) -- exchange U
+ *           halos before it;
+ *   part 2: the corrector, doViscousStep, time += dt -- exchange UP halos
+ *           before it;
+ *   part 3: updatePrims + hrate + cooling, and the CFL minimum of the new
+ *           state.
+ * wx3d_get_dtmin returns this process's CFL minimum (dx/(|v|+c) over its
+ * blocks, computed if needed); wx3d_set_dtmin replaces it with the global
+ * minimum (MPI_ALLREDUCE, hydro_solver.f90:198) before part 0. */
+int wx3d_step_part(wx_ctx* ctx, int32_t part);
+int wx3d_get_dtmin(wx_ctx* ctx, double* dtmin);
+int wx3d_set_dtmin(wx_ctx* ctx, double dtmin);
+
+/* Copies n whole blocks (slots, host array) of the current state (array 0)
+ * or of the predictor state UP (array 1) to a device buffer of
+ * n*neqtot*4096 doubles, block after block in native layout, or back. */
+int wx3d_pack_blocks(wx_ctx* ctx, int32_t array, int32_t n, const int32_t* slots, double* d_buf);
+int wx3d_unpack_blocks(wx_ctx* ctx, int32_t array, int32_t n, const int32_t* slots, const double* d_buf);
 
 /* Human-readable text of a status code and of the context's last error. */
 const char* wx3d_error_string(int32_t code);

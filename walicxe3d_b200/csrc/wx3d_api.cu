@@ -171,6 +171,8 @@ struct wx_ctx {
   int nwork = 0;
   int zsplit = 1;
   bool fuse = true;   // corrector carries the viscous step when zsplit == 1
+  int zero_ghost = 0; // single-stage solver: the viscous step sees zero UP ghosts
+  int nhalo = 0;      // slots that hold copies of other processes' blocks
   int grid_stage = 0, grid_256 = 0;
   bool dt_valid = false;
   bool prestep = false;           // dW holds the state at the start of the last step
@@ -401,14 +403,51 @@ bool fuse_visc(const wx_ctx* c) {
   return c->fuse && c->zsplit == 1 && s != WX_SOLVER_LAX && s != WX_SOLVER_HLL1;
 }
 
+// The first stage: Godunov's predictor (dt/2), or the single stage of HLL1
+// and Lax-Friedrichs (result in W).
+int solver_first(wx_ctx* c) {
+  const int solver = c->cfg.solver_type;
+  int rc;
+  c->zero_ghost = 0;
+  if (solver == WX_SOLVER_LAX) {
+    LaxParams P{c->dU, c->dW, c->dBlocks, c->dWork, c->nwork, c->dCtl, c->ph};
+    tick(c, 1, true);
+    c->k.lax<<<grid_for(c, (const void*)c->k.lax, 256, 0, c->nwork), 256, 0, c->stream>>>(P);
+    WX_LAUNCHED();
+    tick(c, 1, false);
+    c->zero_ghost = 1;
+  } else if (solver == WX_SOLVER_HLL1) {
+    if ((rc = launch_stage(c, 1, c->dU, c->dU, c->dW, 1.0))) return rc;
+    c->zero_ghost = 1;
+  } else {
+    if ((rc = launch_stage(c, 1, c->dU, c->dU, c->dUP, 0.5))) return rc;
+  }
+  return WX_OK;
+}
+
+// The corrector (two-stage solvers), doViscousStep, time += dt, and the
+// U/W swap: on return dU holds U^{n+1}.
+int solver_second(wx_ctx* c, bool finish_output) {
+  const int solver = c->cfg.solver_type;
+  int rc;
+  if (solver != WX_SOLVER_LAX && solver != WX_SOLVER_HLL1 &&
+      (rc = launch_stage(c, 2, c->dUP, c->dU, c->dW, 1.0, fuse_visc(c))))
+    return rc;
+  if (!fuse_visc(c) && (rc = launch_visc(c, c->zero_ghost))) return rc;
+  step_end_kernel<<<1, 1, 0, c->stream>>>(c->dCtl, finish_output ? 1 : 0);
+  WX_LAUNCHED();
+  std::swap(c->dU, c->dW);
+  c->prestep = true;
+  c->dt_valid = !sources_on(c);
+  return WX_OK;
+}
+
 // Godunov(order)/LaxFriedrichs + doViscousStep; on return dU holds U^{n+1}.
 int enqueue_solver(wx_ctx* c, bool bump_it, bool finish_output) {
-  const int solver = c->cfg.solver_type;
   const bool src = sources_on(c);
   step_begin_kernel<<<1, 1, 0, c->stream>>>(c->dCtl, c->ph.cfl, c->cfg.cooling_type != WX_COOL_NONE, c->ph.dtout,
                                             c->ph.t_sc, bump_it ? 1 : 0);
   WX_LAUNCHED();
-  int zero_ghost = 0;
   int rc;
   if (!c->hwind.empty()) {
     // Wind run (userBoundary after every ghost fill, winds.f90:123-240).
@@ -431,27 +470,8 @@ int enqueue_solver(wx_ctx* c, bool bump_it, bool finish_output) {
     c->dt_valid = !src;
     return WX_OK;
   }
-  if (solver == WX_SOLVER_LAX) {
-    LaxParams P{c->dU, c->dW, c->dBlocks, c->dWork, c->nwork, c->dCtl, c->ph};
-    tick(c, 1, true);
-    c->k.lax<<<grid_for(c, (const void*)c->k.lax, 256, 0, c->nwork), 256, 0, c->stream>>>(P);
-    WX_LAUNCHED();
-    tick(c, 1, false);
-    zero_ghost = 1;
-  } else if (solver == WX_SOLVER_HLL1) {
-    if ((rc = launch_stage(c, 1, c->dU, c->dU, c->dW, 1.0))) return rc;
-    zero_ghost = 1;
-  } else {
-    if ((rc = launch_stage(c, 1, c->dU, c->dU, c->dUP, 0.5))) return rc;
-    if ((rc = launch_stage(c, 2, c->dUP, c->dU, c->dW, 1.0, fuse_visc(c)))) return rc;
-  }
-  if (!fuse_visc(c) && (rc = launch_visc(c, zero_ghost))) return rc;
-  step_end_kernel<<<1, 1, 0, c->stream>>>(c->dCtl, finish_output ? 1 : 0);
-  WX_LAUNCHED();
-  std::swap(c->dU, c->dW);
-  c->prestep = true;
-  c->dt_valid = !src;
-  return WX_OK;
+  if ((rc = solver_first(c))) return rc;
+  return solver_second(c, finish_output);
 }
 
 // mode bits: 1 = hrate, 2 = cooling, 4 = read/write the PRIM buffer, 8 = CFL minimum
@@ -673,8 +693,19 @@ int wx3d_set_stream(wx_ctx* c, void* s) {
 
 // Neighbour table from the localBlocks registry (amr.f90:539-631 neighbors,
 // :831 siblingCoords, :916 father, :882 children).
-int wx3d_set_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb) {
-  if (!c || !lb || nslots < 0) return WX_ERR_INVALID_ARG;
+int wx3d_set_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb) { return wx3d_set_mesh_halo(c, nslots, lb, 0, nullptr); }
+
+// As wx3d_set_mesh, with nhalo slots holding copies of blocks another
+// process owns: they are read as neighbours but never updated, and their
+// own faces may lead out of the local block set.
+int wx3d_set_mesh_halo(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nhalo, const int32_t* halo) {
+  if (!c || !lb || nslots < 0 || nhalo < 0 || (nhalo > 0 && !halo)) return WX_ERR_INVALID_ARG;
+  std::vector<char> is_halo(c->max_blocks, 0);
+  for (int h = 0; h < nhalo; ++h) {
+    if (halo[h] < 0 || halo[h] >= nslots || lb[halo[h]] == -1) return fail(c, WX_ERR_INVALID_ARG, "halo slot %d is not an occupied slot", halo[h]);
+    is_halo[halo[h]] = 1;
+  }
+  if (nhalo > 0 && !c->hwind.empty()) return fail(c, WX_ERR_UNSUPPORTED, "wind sources in a partitioned run");
   if (nslots > c->max_blocks) return fail(c, WX_ERR_INSUFICIENT_NBMAXPROC, "%d slots > max_blocks %d", nslots, c->max_blocks);
   const Tree& T = c->tree;
   std::unordered_map<long long, int> slot;
@@ -723,7 +754,10 @@ int wx3d_set_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb) {
       }
       // finer: the four children of nID adjacent to this face, transverse
       // axes in x<y<z order (amr.f90:590-628)
-      if (l >= T.maxlev) return fail(c, WX_ERR_MESH, "bID %lld face %d: no active neighbour", id, f + 1);
+      if (l >= T.maxlev) {
+        if (is_halo[s]) { b.ftype[f] = 0; continue; }   // outside the local set
+        return fail(c, WX_ERR_MESH, "bID %lld face %d: no active neighbour", id, f + 1);
+      }
       const int t1 = ax == 0 ? 1 : 0, t2 = ax == 2 ? 1 : 2;
       b.ftype[f] = WX_NEIGH_FINER;
       for (int q = 0; q < 4; ++q) {
@@ -732,16 +766,19 @@ int wx3d_set_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb) {
         ch[t1] = 2 * y[t1] + (q & 1);
         ch[t2] = 2 * y[t2] + (q >> 1);
         auto ct = slot.find(T.id(l + 1, ch));
-        if (ct == slot.end())
+        if (ct == slot.end()) {
+          if (is_halo[s]) { b.ftype[f] = 0; break; }
           return fail(c, WX_ERR_MESH, "bID %lld face %d: neighbour region is neither same, coarser nor finer by one", id, f + 1);
+        }
         b.fnb[f][q] = ct->second;
       }
     }
     hb[s] = b;
-    work.push_back(s);
+    if (!is_halo[s]) work.push_back(s);
   }
   c->local.assign(c->max_blocks, -1);
   std::copy(lb, lb + nslots, c->local.begin());
+  c->nhalo = nhalo;
   int bad = -1;
   if (!flag_wind_blocks(c, hb, &bad))
     return fail(c, WX_ERR_UNSUPPORTED, "slot %d: a wind sphere reaches the ghost layer of a coarse/fine face; "
@@ -811,6 +848,79 @@ int wx3d_set_winds(wx_ctx* c, int32_t nwind, const wx_wind* winds) {
   WX_CUDA(cudaStreamSynchronize(c->stream));
   invalidate_graph(c);
   return WX_OK;
+}
+
+int wx3d_step_part(wx_ctx* c, int32_t part) {
+  if (!ready(c) || part < 0 || part > 3) return WX_ERR_INVALID_ARG;
+  if (!c->hwind.empty()) return fail(c, WX_ERR_UNSUPPORTED, "the step in parts does not run wind sources");
+  int rc;
+  c->nev = 0;
+  switch (part) {
+    case 0:
+      if (!c->dt_valid) {
+        if ((rc = launch_dt(c, c->dU))) return rc;
+        c->dt_valid = true;
+      }
+      step_begin_kernel<<<1, 1, 0, c->stream>>>(c->dCtl, c->ph.cfl, c->cfg.cooling_type != WX_COOL_NONE, c->ph.dtout,
+                                                c->ph.t_sc, 1);
+      WX_LAUNCHED();
+      return WX_OK;
+    case 1: return solver_first(c);
+    case 2: return solver_second(c, true);
+    default:
+      if (sources_on(c)) {
+        int mode = 8;
+        if (c->cfg.eos_type == WX_EOS_H_RATE) mode |= 1;
+        if (c->cfg.cooling_type != WX_COOL_NONE) mode |= 2;
+        if ((rc = enqueue_sources(c, mode))) return rc;
+      }
+      return sync_check(c);
+  }
+}
+
+int wx3d_get_dtmin(wx_ctx* c, double* v) {
+  if (!ready(c) || !v) return WX_ERR_INVALID_ARG;
+  int rc;
+  if (!c->dt_valid) {
+    if ((rc = launch_dt(c, c->dU))) return rc;
+    c->dt_valid = true;
+  }
+  WX_CUDA(cudaMemcpyAsync(c->hCtl, c->dCtl, sizeof(DevCtl), cudaMemcpyDeviceToHost, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  std::memcpy(v, &c->hCtl->dtmin_bits, 8);
+  return WX_OK;
+}
+
+int wx3d_set_dtmin(wx_ctx* c, double v) {
+  if (!c || !(v > 0.0)) return WX_ERR_INVALID_ARG;
+  unsigned long long bits;
+  std::memcpy(&bits, &v, 8);   // positive doubles order like their bit patterns
+  WX_CUDA(cudaMemcpyAsync(&c->dCtl->dtmin_bits, &bits, 8, cudaMemcpyHostToDevice, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  c->dt_valid = true;
+  return WX_OK;
+}
+
+static int copy_blocks(wx_ctx* c, int32_t array, int32_t n, const int32_t* slots, double* buf, bool pack) {
+  if (!c || n < 0 || (n > 0 && (!slots || !buf)) || (array != 0 && array != 1)) return WX_ERR_INVALID_ARG;
+  double* a = array == 0 ? c->dU : c->dUP;
+  const size_t per = (size_t)c->neq * BCELLS * 8;
+  for (int b = 0; b < n; ++b) {
+    if (slots[b] < 0 || slots[b] >= c->max_blocks) return fail(c, WX_ERR_INVALID_ARG, "slot %d out of range", slots[b]);
+    double* s = a + (size_t)slots[b] * c->neq * BCELLS;
+    double* d = buf + (size_t)b * c->neq * BCELLS;
+    WX_CUDA(cudaMemcpyAsync(pack ? d : s, pack ? s : d, per, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  return WX_OK;
+}
+
+int wx3d_pack_blocks(wx_ctx* c, int32_t array, int32_t n, const int32_t* slots, double* d_buf) {
+  return copy_blocks(c, array, n, slots, d_buf, true);
+}
+
+int wx3d_unpack_blocks(wx_ctx* c, int32_t array, int32_t n, const int32_t* slots, const double* d_buf) {
+  return copy_blocks(c, array, n, slots, const_cast<double*>(d_buf), false);
 }
 
 int wx3d_set_fusion(wx_ctx* c, int32_t on) {
