@@ -109,6 +109,8 @@ typedef struct wx_config {
   int32_t bc[6];             /* bc_left, bc_right, bc_front, bc_back, bc_bottom, bc_top */
   int32_t eight_wave;        /* Powell 8-wave source (brio-wu/parameters.f90:198) */
   int32_t user_source_terms; /* must be 0: get_user_source_terms is not part of this ABI */
+  int32_t enable_flux_cd;    /* field-CD update of B (brio-wu/parameters.f90:200, brio-wu/flux_cd.f90:52-86) */
+  int32_t pad0;              /* keeps the doubles 8-byte aligned; set to 0 */
   int32_t nbrootx, nbrooty, nbrootz; /* root blocks (MESH_MANUAL)        */
   int32_t maxlev;            /* number of refinement levels              */
   double gamma;              /* heat capacity ratio                      */

@@ -760,10 +760,58 @@ void source_function(const Ctx& c, int nb, int lev, int i, int j, int k, double*
   }
 }
 
-// upwindStep (godunov.f90:199-277)
+// flux_cd_update (brio-wu/flux_cd.f90:52-86) for every physical cell of a
+// block.  The reference declares efield(3,0:n+1,0:n+1,0:n+1) (flux_cd.f90:37)
+// but never fills it and never calls flux_cd_update; the restatement fills
+// efield with the field-interpolated electric field E = -v x B of the
+// primitives the fluxes were computed from (Toth 2000, J. Comput. Phys. 161,
+// 605, field-CD scheme).  As in flux_cd_update, no source term is added.
+void flux_cd_update(Ctx& c, int nb, double dtdx, double dtdy, double dtdz, const Fluxes& F) {
+  constexpr int NE = NC + 2;
+  std::vector<double> ef(3 * NE * NE * NE);
+  auto E = [&](int d, int i, int j, int k) -> double& { return ef[((size_t)(d * NE + k) * NE + j) * NE + i]; };
+  auto P = [&](int e, int i, int j, int k) { return c.u(c.PRIM, nb, e)[cidx(i, j, k)]; };
+  for (int k = 0; k <= NC + 1; ++k)
+    for (int j = 0; j <= NC + 1; ++j)
+      for (int i = 0; i <= NC + 1; ++i) {
+        const double v1 = P(1, i, j, k), v2 = P(2, i, j, k), v3 = P(3, i, j, k);
+        const double b1 = P(5, i, j, k), b2 = P(6, i, j, k), b3 = P(7, i, j, k);
+        E(0, i, j, k) = v3 * b2 - v2 * b3;
+        E(1, i, j, k) = v1 * b3 - v3 * b1;
+        E(2, i, j, k) = v2 * b1 - v1 * b2;
+      }
+  for (int i = 1; i <= NC; ++i)
+    for (int j = 1; j <= NC; ++j)
+      for (int k = 1; k <= NC; ++k) {
+        for (int e = 0; e < c.neq; ++e) {
+          if (e >= 5 && e <= 7) continue;
+          const double* fc = F.FC.data() + (size_t)e * NCELL;
+          const double* gc = F.GC.data() + (size_t)e * NCELL;
+          const double* hc = F.HC.data() + (size_t)e * NCELL;
+          c.u(c.UP, nb, e)[cidx(i, j, k)] = c.u(c.U, nb, e)[cidx(i, j, k)] -
+                                            dtdx * (fc[cidx(i, j, k)] - fc[cidx(i - 1, j, k)]) -
+                                            dtdy * (gc[cidx(i, j, k)] - gc[cidx(i, j - 1, k)]) -
+                                            dtdz * (hc[cidx(i, j, k)] - hc[cidx(i, j, k - 1)]);
+        }
+        auto U = [&](int e) { return c.u(c.U, nb, e)[cidx(i, j, k)]; };
+        c.u(c.UP, nb, 5)[cidx(i, j, k)] = U(5) - 0.5 * dtdy * (E(2, i, j + 1, k) - E(2, i, j - 1, k)) -
+                                          0.5 * dtdz * (-E(1, i, j, k + 1) + E(1, i, j, k - 1));
+        c.u(c.UP, nb, 6)[cidx(i, j, k)] = U(6) - 0.5 * dtdx * (-E(2, i + 1, j, k) + E(2, i - 1, j, k)) -
+                                          0.5 * dtdz * (E(0, i, j, k + 1) - E(0, i, j, k - 1));
+        c.u(c.UP, nb, 7)[cidx(i, j, k)] = U(7) - 0.5 * dtdx * (E(1, i + 1, j, k) - E(1, i - 1, j, k)) -
+                                          0.5 * dtdy * (-E(0, i, j + 1, k) + E(0, i, j - 1, k));
+      }
+}
+
+// upwindStep (godunov.f90:199-277); with enable_flux_cd the update is
+// flux_cd_update's
 void upwindStep(Ctx& c, int nb, double dtp, const Fluxes& F) {
   int lev = meshlevel(c, c.localBlocks[nb]);
   double dtdx = dtp / c.dx[lev], dtdy = dtp / c.dy[lev], dtdz = dtp / c.dz[lev];
+  if (c.cfg.enable_flux_cd) {
+    flux_cd_update(c, nb, dtdx, dtdy, dtdz, F);
+    return;
+  }
   const bool src = c.cfg.eight_wave || c.cfg.user_source_terms;
   double s[MAXEQ];
   for (int i = 1; i <= NC; ++i)

@@ -30,7 +30,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_struct_sizes_match_header():
     # wx_config: 17 int32 fields (+ 5 for bc[6] beyond one) then 17 doubles
-    assert ctypes.sizeof(WxConfig) == 4 * 20 + 8 * 17
+    assert ctypes.sizeof(WxConfig) == 4 * 22 + 8 * 17
     assert ctypes.sizeof(WxState) == 32
     assert ctypes.sizeof(WxStatus) == 64
 
@@ -72,6 +72,16 @@ def test_unsupported_configs_rejected_before_device_use():
     lib.wx3d_config_defaults(ctypes.byref(c))
     c.eos_type = 3  # H_RATE needs a passive scalar
     assert lib.wx3d_init(ctypes.byref(c), 8, ctypes.byref(h)) == 26
+    # the field-CD update of B needs an active field, excludes the 8-wave
+    # source and applies to the Godunov solvers only
+    lib.wx3d_config_defaults(ctypes.byref(c))
+    c.enable_flux_cd = 1
+    assert lib.wx3d_init(ctypes.byref(c), 8, ctypes.byref(h)) == 104
+    c.bfield, c.mhd, c.neqtot, c.npassive, c.solver_type = 1, 1, 8, 0, 6  # HLLD
+    c.eight_wave = 1
+    assert lib.wx3d_init(ctypes.byref(c), 8, ctypes.byref(h)) == 104
+    c.eight_wave, c.solver_type = 0, 1  # Lax-Friedrichs
+    assert lib.wx3d_init(ctypes.byref(c), 8, ctypes.byref(h)) == 104
 
 
 def test_package_has_no_cpu_fallback(tmp_path):

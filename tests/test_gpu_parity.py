@@ -491,3 +491,39 @@ def test_cooling_variants_match_oracle(ctype, ncpu):
         g.step()
     check(o, g, prob)
     assert g.download()[:, 4].sum() < (1.0 - 1e-4) * E0
+
+
+@pytest.mark.parametrize("shape", ["1-fused", "1", "2", "8"])
+@pytest.mark.parametrize("solver", [C.SOLVER_HLLD, C.SOLVER_HLL1])
+def test_field_cd_matches_oracle(shape, solver, ncpu):
+    """The field-CD update of B (brio-wu/flux_cd.f90:52-86 with E = -v x B of
+    the stage primitives) against the oracle on the 3-D Orszag-Tang vortex,
+    in every launch shape (the carried E of the plane below crosses z-slab
+    boundaries), for the two-stage and the first-order solver."""
+    prob = problems.orszag_tang_3d(nroot=2, solver=solver)
+    o = oracle.from_problem(prob, threads=ncpu)
+    g = from_problem(prob)
+    _shape(g, shape)
+    for _ in range(12):
+        o.step()
+        g.step()
+    check(o, g, prob)
+
+
+def test_field_cd_keeps_the_central_divergence_on_the_gpu():
+    """4^3 blocks of the 3-D Orszag-Tang vortex, 20 steps through the CUDA
+    graph: the central-difference divergence of B stays at its initial value
+    to round-off with field-CD, and drifts with the 8-wave source."""
+    from divergence import central_divergence
+    drift = {}
+    for flux_cd in (True, False):
+        prob = problems.orszag_tang_3d(nroot=4, flux_cd=flux_cd)
+        g = from_problem(prob)
+        d0 = central_divergence(prob, g.download())
+        g.run(20)
+        U = g.download()
+        assert np.all(np.isfinite(U))
+        drift[flux_cd] = np.abs(central_divergence(prob, U) - d0).max()
+        scale = np.abs(d0).max()
+    assert drift[True] <= 1e-12 * scale
+    assert drift[False] >= 1e-3 * scale

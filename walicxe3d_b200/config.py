@@ -53,6 +53,8 @@ class WxConfig(ctypes.Structure):
         ("bc", ctypes.c_int32 * 6),
         ("eight_wave", ctypes.c_int32),
         ("user_source_terms", ctypes.c_int32),
+        ("enable_flux_cd", ctypes.c_int32),
+        ("pad0", ctypes.c_int32),
         ("nbrootx", ctypes.c_int32),
         ("nbrooty", ctypes.c_int32),
         ("nbrootz", ctypes.c_int32),
@@ -119,6 +121,7 @@ class Config:
     cooling_type: int = COOL_NONE
     bc: tuple = (BC_FREE_FLOW,) * 6
     eight_wave: bool = False
+    enable_flux_cd: bool = False
     nbroot: tuple = (1, 1, 1)
     maxlev: int = 1
     gamma: float = 5.0 / 3.0
@@ -177,6 +180,7 @@ class Config:
             c.bc[i] = self.bc[i]
         c.eight_wave = int(self.eight_wave)
         c.user_source_terms = 0
+        c.enable_flux_cd = int(self.enable_flux_cd)
         c.nbrootx, c.nbrooty, c.nbrootz = self.nbroot
         c.maxlev = self.maxlev
         c.gamma = self.gamma

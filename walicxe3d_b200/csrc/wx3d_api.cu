@@ -227,6 +227,11 @@ int validate(const wx_config& f, std::string& why) {
   if (f.mhd && !f.bfield) { why = "mhd without bfield computes no time step in the reference"; return WX_ERR_UNSUPPORTED; }
   if (f.bfield && !f.mhd) { why = "passive magnetic field (bfield without mhd) is not supported"; return WX_ERR_UNSUPPORTED; }
   if (f.user_source_terms) { why = "user source terms are not part of this ABI"; return WX_ERR_UNSUPPORTED; }
+  if (f.enable_flux_cd) {
+    if (!(f.bfield && f.mhd)) { why = "enable_flux_cd needs an active magnetic field (bfield and mhd)"; return WX_ERR_UNSUPPORTED; }
+    if (f.eight_wave) { why = "enable_flux_cd and eight_wave are alternative div(B) controls (init.f90:264-270): pick one"; return WX_ERR_UNSUPPORTED; }
+    if (f.solver_type == WX_SOLVER_LAX) { why = "the field-CD update replaces upwindStep, which the Lax-Friedrichs solver does not use"; return WX_ERR_UNSUPPORTED; }
+  }
   for (int i = 0; i < 6; ++i) {
     if (f.bc[i] == WX_BC_PERIODIC) { why = "BC_PERIODIC is not implemented by the reference (ghosts stay stale)"; return WX_ERR_UNSUPPORTED; }
     if (f.bc[i] != WX_BC_REFLECTIVE && f.bc[i] != WX_BC_FREE_FLOW) { why = "unknown boundary condition"; return WX_ERR_INVALID_ARG; }
@@ -253,6 +258,7 @@ void fill_phys(wx_ctx* c) {
   p.cooling_limit = f.cooling_limit;
   p.limiter = f.limiter_type;
   p.eight_wave = f.eight_wave;
+  p.flux_cd = f.enable_flux_cd;
   for (int i = 0; i < 6; ++i) p.bc[i] = f.bc[i];
   p.eos = f.eos_type;
   p.cooling = f.cooling_type;
@@ -1768,6 +1774,7 @@ void noalloc_phys(const wx_config& f, PhysParams& p) {
   p.cooling_limit = f.cooling_limit;
   p.limiter = f.limiter_type;
   p.eight_wave = f.eight_wave;
+  p.flux_cd = f.enable_flux_cd;
   for (int i = 0; i < 6; ++i) p.bc[i] = f.bc[i];
   p.eos = f.eos_type;
   p.cooling = f.cooling_type;

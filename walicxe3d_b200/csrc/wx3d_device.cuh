@@ -57,6 +57,7 @@ struct PhysParams {
   double cooling_limit;
   int32_t limiter;
   int32_t eight_wave;
+  int32_t flux_cd;   // field-CD update of B (brio-wu/flux_cd.f90:52-86)
   int32_t bc[6];
   int32_t eos;
   int32_t cooling;

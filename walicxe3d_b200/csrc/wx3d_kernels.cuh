@@ -222,6 +222,19 @@ __host__ __device__ constexpr int stage_ctas_per_sm() {
   return (!MHD && 2 * (stage_smem_bytes<NEQ, MHD, ORDER, VISC>() + 1024) <= 228 * 1024) ? 2 : 1;
 }
 
+// Cell-centred electric field E = -v x B of the stage primitives at one ring
+// cell: the field-interpolated E of the field-CD scheme (Toth 2000, J. Comput.
+// Phys. 161, 605), which brio-wu/flux_cd.f90:37 declares as efield(3,...).
+template <int ORDER>
+__device__ __forceinline__ void efield(const double* c, double* E) {
+  constexpr int PL = Geo<ORDER>::PL;
+  const double v1 = c[1 * PL], v2 = c[2 * PL], v3 = c[3 * PL];
+  const double b1 = c[5 * PL], b2 = c[6 * PL], b3 = c[7 * PL];
+  E[0] = v3 * b2 - v2 * b3;
+  E[1] = v1 * b3 - v3 * b1;
+  E[2] = v2 * b1 - v1 * b2;
+}
+
 template <int NEQ, bool MHD, int SOLVER, int ORDER, int LIM, bool VISC = false>
 __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, ORDER, VISC>())) stage_kernel(StageParams P) {
   constexpr int CH = ring_channels<NEQ, MHD, ORDER>();
@@ -253,6 +266,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) { zprev[e] = 0.0; znew[e] = 0.0; zslope[e] = 0.0; }
     double bz_below = 0.0;  // B_z of plane m-1 in this thread's column (Powell source)
+    double e_below[3] = {0.0, 0.0, 0.0};  // E of plane m-1 in this thread's column (field-CD)
 
     // ---- prologue: planes z0-ORDER .. z0+ORDER-1, the z-interface z0-1/2,
     // then plane z0+ORDER into the slot of plane z0-ORDER ------------------
@@ -266,6 +280,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
       const double* c3 = ring + ring_slot(m + 2) * CH * Geo<ORDER>::PL + hc;
       iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 2, true>(c0, c1, c2, c3, ph, znew, zslope, true);
       if (MHD) bz_below = c1[7 * Geo<ORDER>::PL];
+      if (MHD && ph.flux_cd) efield<ORDER>(c1, e_below);
     }
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) zprev[e] = znew[e];
@@ -348,6 +363,26 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
         }
         if (MHD) bz_below = ring[ring_slot(m) * CH * Geo<ORDER>::PL + 7 * Geo<ORDER>::PL + hc];
         const size_t o = cell_off(slot, NEQ, 0, ci, cj, m);
+        // field-CD (brio-wu/flux_cd.f90:74-84): B from the central differences
+        // of E over the six face neighbours; E of plane m-1 is carried
+        double bcd[3] = {0.0, 0.0, 0.0};
+        if (MHD && ph.flux_cd) {
+          constexpr int PL = Geo<ORDER>::PL, W = Geo<ORDER>::W;
+          const double* pm = ring + ring_slot(m) * CH * PL + hc;
+          double xl[3], xr[3], yl[3], yr[3], zu[3], ec[3];
+          efield<ORDER>(pm - 1, xl);
+          efield<ORDER>(pm + 1, xr);
+          efield<ORDER>(pm - W, yl);
+          efield<ORDER>(pm + W, yr);
+          efield<ORDER>(ring + ring_slot(m + 1) * CH * PL + hc, zu);
+          efield<ORDER>(pm, ec);
+          const double hx = 0.5 * dtdx, hy = 0.5 * dtdy, hz = 0.5 * dtdz;
+          bcd[0] = __ldg(P.base + o + 5 * (size_t)BCELLS) - hy * (yr[2] - yl[2]) - hz * (-zu[1] + e_below[1]);
+          bcd[1] = __ldg(P.base + o + 6 * (size_t)BCELLS) - hx * (-xr[2] + xl[2]) - hz * (zu[0] - e_below[0]);
+          bcd[2] = __ldg(P.base + o + 7 * (size_t)BCELLS) - hx * (xr[1] - xl[1]) - hy * (-yr[0] + yl[0]);
+#pragma unroll
+          for (int d = 0; d < 3; ++d) e_below[d] = ec[d];
+        }
         double wv[NEQ];
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) {
@@ -356,6 +391,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
           double v = __ldg(P.base + o + (size_t)e * BCELLS) + dtdx * (fxl - fxr) + dtdy * (fyl - fyr) +
                      dtdz * (zprev[e] - znew[e]);
           if (MHD && ph.eight_wave) v = v + dtp * s[e];
+          if (MHD && ph.flux_cd && e >= 5 && e <= 7) v = bcd[e - 5];
           if (VISC) wv[e] = v;
           else P.out[o + (size_t)e * BCELLS] = v;
         }
