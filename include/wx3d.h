@@ -15,6 +15,7 @@
  *   markByPhysical(...)      source/amr.f90:142           -> wx3d_mark
  *   refineBlock(fatherID)    source/amr.f90:284 (data)    -> wx3d_refine
  *   coarseBlocks()           source/amr.f90:1430 (data)   -> wx3d_coarsen
+ *   admesh()                 source/amr.f90:44            -> wx3d_admesh
  *   main-loop body           source/main.f90:81-100       -> wx3d_step / wx3d_run
  *
  * Memory: the library owns the device copies of every block's conserved
@@ -74,7 +75,9 @@ enum { WX_COOL_NONE = 0, WX_COOL_TABLE = 1, WX_COOL_TABLE_METAL = 2, WX_COOL_H =
 enum {
   WX_OK = 0,
   WX_ERR_GENERIC = 255,
+  WX_ERR_ALREADY_MAX_LEV = 6,
   WX_ERR_INSUFICIENT_NBMAXPROC = 7,
+  WX_ERR_REGISTER_FATHER = 10,
   WX_ERR_TOO_MANY_LEVS = 12,
   WX_ERR_COOLING_LOAD_COEFS = 14,
   WX_ERR_OUTPUT_FILE_OPEN = 18,
@@ -312,6 +315,22 @@ int wx3d_refine(wx_ctx* ctx, int32_t father_slot, const int32_t* child_slots8);
 /* Data part of coarseBlocks (source/amr.f90:1597-1625): 8-cell averages of
  * the 8 siblings (natural order) into the father slot. */
 int wx3d_coarsen(wx_ctx* ctx, const int32_t* child_slots8, int32_t father_slot);
+
+/* admesh (source/amr.f90:44-133) of one process, in place of the whole
+ * subroutine: markByPhysical on the device, checkProximity(maxlev-1)
+ * (amr.f90:1109-1254) on the flags, refineBlock (:284-384) for every block
+ * still marked REFINE in slot order, then coarseBlocks (:1430-1650) for
+ * every family whose eight siblings are marked COARSE.  Slots follow the
+ * reference's registry: a new block takes the first empty slot (put,
+ * utils.f90:112) and a removed block frees its own (pop, :157); with one
+ * process loadBalance moves no block, so the slot order is the reference's.
+ * local_blocks (nbmax = the context's max_blocks entries, -1 = empty) must
+ * hold the list last passed to wx3d_set_mesh, padded with -1; on return it
+ * holds the new list and the device neighbour table is rebuilt from it.
+ * counts2 (may be NULL): blocks refined, families coarsened.  Capacity
+ * errors (WX_ERR_INSUFICIENT_NBMAXPROC, WX_ERR_REGISTER_FATHER) are found
+ * before any data moves and leave the mesh and the state unchanged. */
+int wx3d_admesh(wx_ctx* ctx, int32_t nbmax, int32_t* local_blocks, int32_t* counts2);
 
 /* Per-kernel device timing with CUDA events recorded around each launch of
  * the step sequence (inside the CUDA graph of wx3d_run).  wx3d_kernel_times

@@ -70,6 +70,8 @@ def load() -> ctypes.CDLL:
             "orc_mark": (None, [vp, ip]),
             "orc_refine": (None, [vp, ctypes.c_int, ip]),
             "orc_coarsen": (None, [vp, ip, ctypes.c_int]),
+            "orc_admesh": (ctypes.c_int, [vp, ip]),
+            "orc_get_blocks": (None, [vp, ip]),
         }
         for n, (r, a) in sig.items():
             f = getattr(lib, n)
@@ -204,6 +206,22 @@ class Oracle:
     def coarsen(self, children, father):
         c = np.ascontiguousarray(children, dtype=np.int32)
         self.lib.orc_coarsen(self.h, _ip(c), int(father))
+
+    def admesh(self):
+        """admesh (amr.f90:44-133) with one process; returns (blocks refined,
+        families coarsened).  Raises on the reference's abort codes."""
+        n = np.zeros(2, np.int32)
+        rc = self.lib.orc_admesh(self.h, _ip(n))
+        if rc:
+            raise RuntimeError(f"oracle admesh aborted with code {rc}")
+        return int(n[0]), int(n[1])
+
+    @property
+    def blocks(self) -> np.ndarray:
+        """localBlocks (nbmax entries, -1 = empty slot)."""
+        b = np.zeros(self.nbmax, np.int32)
+        self.lib.orc_get_blocks(self.h, _ip(b))
+        return b
 
     def neighbors(self, bid: int, direction: int):
         t = ctypes.c_int()

@@ -1488,6 +1488,151 @@ int markByPhysical(const Ctx& c, int nb) {  // amr.f90:142-230
   return WX_FLAG_NONE;
 }
 
+// Registry helpers (utils.f90:78-172): linear find, put into the first
+// empty slot, pop.
+int find(const std::vector<int>& list, int element) {
+  for (int nb = 0; nb < (int)list.size(); ++nb)
+    if (list[nb] == element) return nb;
+  return -1;
+}
+int put(std::vector<int>& list, int element) {
+  int nb = find(list, -1);
+  if (nb != -1) list[nb] = element;
+  return nb;
+}
+int pop(std::vector<int>& list, int element) {
+  int nb = find(list, element);
+  if (nb != -1) list[nb] = -1;
+  return nb;
+}
+
+// checkProximity (amr.f90:1109-1254) with globalBlocks = localBlocks (one
+// process); refineFlags change while the sweep goes.
+void checkProximity(const Ctx& c, std::vector<int>& refineFlags, int finestLev) {
+  const std::vector<int>& globalBlocks = c.localBlocks;
+  for (int level = finestLev; level >= 1; --level)
+    for (int nb = 0; nb < c.nbMax; ++nb) {
+      int bID = globalBlocks[nb];
+      if (bID == -1 || bID < c.minID[level] || bID > c.maxID[level]) continue;
+      int bflag = refineFlags[nb];
+      if (bflag == WX_FLAG_REFINE) {
+        for (int dir = 1; dir <= 6; ++dir) {
+          int ntype, list[4];
+          neighbors(c, bID, dir, ntype, list);
+          if (ntype == WX_NEIGH_SAME) {
+            int nb1 = find(globalBlocks, list[0]);
+            if (refineFlags[nb1] == WX_FLAG_COARSE) refineFlags[nb1] = WX_FLAG_NONE;
+          } else if (ntype == WX_NEIGH_COARSER) {
+            int nb2 = find(globalBlocks, list[0]);
+            if (refineFlags[nb2] != WX_FLAG_REFINE) refineFlags[nb2] = WX_FLAG_REFINE;
+          }
+        }
+      }
+      if (bflag == WX_FLAG_COARSE) {
+        bool inhibited = false;
+        for (int dir = 1; dir <= 6; ++dir) {
+          int ntype, list[4];
+          neighbors(c, bID, dir, ntype, list);
+          if (ntype == WX_NEIGH_FINER) {
+            int sib[8];
+            siblings(c, list[0], sib);
+            for (int i = 0; i < 8; ++i) {
+              int nb1 = find(globalBlocks, sib[i]);
+              if (nb1 != -1 && refineFlags[nb1] != WX_FLAG_COARSE) {
+                refineFlags[nb] = WX_FLAG_NONE;
+                inhibited = true;
+                break;
+              }
+            }
+          }
+          if (inhibited) break;
+        }
+      }
+    }
+}
+
+// refineBlock (amr.f90:284-384): children into the first empty slots, U and
+// PRIM injected from the father, the father's slot freed.
+int refineBlock(Ctx& c, int fatherID, int& nbLocal) {
+  int fatherIndex = find(c.localBlocks, fatherID);
+  if (fatherIndex == -1) return 5;  // ERROR_LOCAL_BID_NOT_FOUND
+  if (meshlevel(c, fatherID) == c.cfg.maxlev) return WX_ERR_ALREADY_MAX_LEV;
+  if (nbLocal + 8 > c.nbMax) return WX_ERR_INSUFICIENT_NBMAXPROC;
+  int childList[8];
+  children(c, fatherID, childList);
+  for (int ch = 0; ch < 8; ++ch) {
+    int childIndex = put(c.localBlocks, childList[ch]);
+    if (childIndex == -1) return 8;  // ERROR_REGISTER_CHILD
+    int sx, sy, sz;
+    siblingCoords(c, childList[ch], sx, sy, sz);
+    for (int i = 1; i <= NC; ++i)
+      for (int j = 1; j <= NC; ++j)
+        for (int k = 1; k <= NC; ++k) {
+          int ip = (NC / 2) * sx + (i + 1) / 2, jp = (NC / 2) * sy + (j + 1) / 2, kp = (NC / 2) * sz + (k + 1) / 2;
+          for (int e = 0; e < c.neq; ++e) {
+            c.u(c.U, childIndex, e)[cidx(i, j, k)] = c.u(c.U, fatherIndex, e)[cidx(ip, jp, kp)];
+            c.u(c.PRIM, childIndex, e)[cidx(i, j, k)] = c.u(c.PRIM, fatherIndex, e)[cidx(ip, jp, kp)];
+          }
+        }
+  }
+  pop(c.localBlocks, fatherID);
+  nbLocal = nbLocal + 7;
+  return 0;
+}
+
+// coarseBlocks (amr.f90:1430-1650), single-process branch: families of
+// marked blocks, then for each family of eight the father takes the first
+// empty slot and receives the 8-cell sums / 8 of every sibling, whose slot
+// is freed; calcPrimsBlock(CELLS_PHYS) of the father.
+int coarseBlocks(Ctx& c, const std::vector<int>& refineFlags, int& ncoarse) {
+  std::vector<std::pair<int, int>> family;
+  for (int nb = 0; nb < c.nbMax; ++nb) {
+    int flag = refineFlags[nb], bID = c.localBlocks[nb];
+    if (bID != -1 && flag == WX_FLAG_COARSE) {
+      int sib[8];
+      siblings(c, bID, sib);
+      int eID = sib[0];
+      bool counted = false;
+      for (auto& f : family)
+        if (f.first == eID) { f.second += 1; counted = true; break; }
+      if (!counted) family.push_back({eID, 1});
+    }
+  }
+  ncoarse = 0;
+  for (auto& f : family) {
+    if (f.second != 8) continue;
+    int eID = f.first, sib[8];
+    siblings(c, eID, sib);
+    int fID = father(c, eID);
+    int fatherIndex = put(c.localBlocks, fID);
+    if (fatherIndex == -1) return WX_ERR_REGISTER_FATHER;
+    for (int s = 0; s < 8; ++s) {
+      int sx, sy, sz;
+      siblingCoords(c, sib[s], sx, sy, sz);
+      int locIndx = find(c.localBlocks, sib[s]);
+      for (int i = 1; i <= NC / 2; ++i)
+        for (int j = 1; j <= NC / 2; ++j)
+          for (int k = 1; k <= NC / 2; ++k) {
+            int i1 = i * 2 - 1, j1 = j * 2 - 1, k1 = k * 2 - 1;
+            int ip = i + sx * NC / 2, jp = j + sy * NC / 2, kp = k + sz * NC / 2;
+            for (int e = 0; e < c.neq; ++e) {
+              const double* src = c.u(c.U, locIndx, e);
+              double sum = 0.0;
+              for (int kk = k1; kk <= k1 + 1; ++kk)
+                for (int jj = j1; jj <= j1 + 1; ++jj)
+                  for (int ii = i1; ii <= i1 + 1; ++ii) sum += src[cidx(ii, jj, kk)];
+              c.u(c.U, fatherIndex, e)[cidx(ip, jp, kp)] = sum / 8.0;
+            }
+          }
+      pop(c.localBlocks, sib[s]);
+    }
+    long long pf = 0, df = 0, zd = 0;
+    calcPrimsBlock(c, c.U, c.PRIM, fatherIndex, CELLS_PHYS, pf, df, zd);
+    ++ncoarse;
+  }
+  return 0;
+}
+
 void setupGeometry(Ctx& c) {  // init.f90:632-756 (MESH_MANUAL)
   const wx_config& f = c.cfg;
   for (int ilev = 1; ilev <= f.maxlev; ++ilev) {
@@ -1700,6 +1845,40 @@ void orc_refine(void* h, int father_slot, const int* child_slots) {
           }
         }
   }
+}
+
+// admesh (amr.f90:44-133) with one process: markByPhysical, checkProximity
+// (maxlev-1), refineBlock for the marked blocks in slot order, coarseBlocks.
+// counts2 = blocks refined, families coarsened.  Returns the reference's
+// abort code (0 = ok).
+int orc_admesh(void* h, int* counts2) {
+  Ctx* c = static_cast<Ctx*>(h);
+  std::vector<int> refineFlags(c->nbMax, WX_FLAG_NONE);
+  for (int nb = 0; nb < c->nbMax; ++nb)
+    if (c->localBlocks[nb] != -1) refineFlags[nb] = markByPhysical(*c, nb);
+  checkProximity(*c, refineFlags, c->cfg.maxlev - 1);
+  const std::vector<int> globalBlocks = c->localBlocks;
+  int nbLocal = 0;
+  for (int b : c->localBlocks) nbLocal += (b != -1);
+  int nref = 0;
+  for (int nb = 0; nb < c->nbMax; ++nb) {
+    if (refineFlags[nb] != WX_FLAG_REFINE) continue;
+    int rc = refineBlock(*c, globalBlocks[nb], nbLocal);
+    if (rc) return rc;
+    ++nref;
+  }
+  int ncoarse = 0;
+  int rc = coarseBlocks(*c, refineFlags, ncoarse);
+  c->slotOf.clear();
+  for (int i = 0; i < c->nbMax; ++i)
+    if (c->localBlocks[i] != -1) c->slotOf[c->localBlocks[i]] = i;
+  if (counts2) { counts2[0] = nref; counts2[1] = ncoarse; }
+  return rc;
+}
+
+void orc_get_blocks(void* h, int* out) {
+  Ctx* c = static_cast<Ctx*>(h);
+  std::copy(c->localBlocks.begin(), c->localBlocks.end(), out);
 }
 
 // coarseBlocks local branch (amr.f90:1592-1625), then calcPrimsBlock(CELLS_PHYS).

@@ -527,3 +527,54 @@ def test_field_cd_keeps_the_central_divergence_on_the_gpu():
         scale = np.abs(d0).max()
     assert drift[True] <= 1e-12 * scale
     assert drift[False] >= 1e-3 * scale
+
+
+def test_admesh_matches_oracle(ncpu):
+    """Live mesh: 12 main-loop steps past the dt ramp, each followed by admesh
+    (amr.f90:44-133) on the device context and in the oracle.  The same
+    blocks refine and coarsen into the same slots (first empty slot, as the
+    reference's put), including slots freed earlier in the same call, and the
+    state after the last step matches."""
+    prob = problems.amr_pulse()
+    extra = 4 * prob.nblocks
+    o = oracle.from_problem(prob, threads=ncpu, extra_slots=extra)
+    g = from_problem(prob, extra_slots=extra)
+    o.set_state(0.0, 0.0, 10, 1, 0)
+    g.set_state(time=0.0, dt=0.0, it=10, nextout=1)
+    total = np.zeros(2, int)
+    for _ in range(12):
+        o.step()
+        g.step()
+        no, ng = o.admesh(), g.admesh()
+        assert no == ng
+        assert np.array_equal(o.blocks, g.local_blocks)
+        total += ng
+    assert total[0] >= 5 and total[1] >= 5
+    occ = g.local_blocks != -1
+    Ug, Uo = g.download(g.max_blocks)[occ], o.U[occ]
+    assert np.all(np.isfinite(Ug))
+    err = rel_l1(Ug, Uo)
+    assert err.max() <= TOL, f"rel L1 per eq {err}"
+    so, sg = o.state, g.state
+    assert sg.it == so.it and sg.time == pytest.approx(so.time, rel=1e-12)
+
+
+def test_admesh_refuses_when_slots_run_out():
+    """Too few free slots for the refinements: WX_ERR_INSUFICIENT_NBMAXPROC
+    before any data moves; the block list and the state stay as they were.
+    A list that differs from the mesh last set is refused too."""
+    from walicxe3d_b200._lib import WxError
+    prob = problems.amr_pulse()
+    g = from_problem(prob, extra_slots=4)
+    g.set_state(time=0.0, dt=0.0, it=10, nextout=1)
+    g.step()
+    U0, lb0 = g.download(g.max_blocks), g.local_blocks.copy()
+    with pytest.raises(WxError) as e:
+        g.admesh()
+    assert e.value.code == 7
+    assert np.array_equal(g.local_blocks, lb0)
+    assert np.array_equal(g.download(g.max_blocks), U0)
+    g.local_blocks = lb0[::-1].copy()
+    with pytest.raises(WxError) as e:
+        g.admesh()
+    assert e.value.code == 106

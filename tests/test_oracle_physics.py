@@ -137,3 +137,37 @@ def test_field_cd_keeps_the_central_divergence(ncpu):
     assert scale > 0.1                       # the initial field is not divergence-free
     assert drift[True] <= 1e-12 * scale
     assert drift[False] >= 1e-3 * scale
+
+
+def test_admesh_keeps_mass_balance_and_cover(ncpu):
+    """admesh (amr.f90:44-133) in the oracle on the live-mesh pulse: the
+    first call coarsens the quiet families and refines around the pulse, a
+    later one follows the spreading pulse; every mesh covers the box once,
+    face neighbours differ by at most one level, and neither the injection
+    nor the 8-cell averaging changes the total mass beyond round-off."""
+    from walicxe3d_b200.partition import face_neighbours
+    prob = problems.amr_pulse()
+    tree = prob.tree
+    o = oracle.from_problem(prob, threads=ncpu, extra_slots=4 * prob.nblocks)
+    o.set_state(0.0, 0.0, 10, 1, 0)   # past the dt ramp
+
+    def mass():
+        U = o.U
+        return sum(U[s, 0].sum() * 8.0 ** (1 - tree.level(int(b))) for s, b in enumerate(o.blocks) if b != -1)
+
+    total = np.zeros(2, int)
+    for _ in range(8):
+        o.step()
+        m0 = mass()
+        n = o.admesh()
+        if n == (0, 0):
+            continue
+        total += n
+        assert abs(mass() - m0) <= 1e-13 * m0
+        leaves = {int(b) for b in o.blocks if b != -1}
+        assert len(leaves) == int((o.blocks != -1).sum())
+        assert sum(8.0 ** (1 - tree.level(b)) for b in leaves) == pytest.approx(8.0, rel=1e-15)
+        for b in leaves:
+            for n in face_neighbours(tree, leaves, b):
+                assert abs(tree.level(n) - tree.level(b)) <= 1
+    assert total[0] >= 5 and total[1] >= 5

@@ -64,6 +64,7 @@ _SIGNATURES = {
     "wx3d_mark": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_int32_p]),
     "wx3d_refine": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_int32_p]),
     "wx3d_coarsen": (ctypes.c_int, [c_void_p, c_int32_p, ctypes.c_int32]),
+    "wx3d_admesh": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_int32_p, c_int32_p]),
     "wx3d_set_timing": (ctypes.c_int, [c_void_p, ctypes.c_int32]),
     "wx3d_kernel_times": (ctypes.c_int, [c_void_p, c_double_p, c_int32_p]),
     "wx3d_get_status": (ctypes.c_int, [c_void_p, ctypes.POINTER(WxStatus)]),

@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <set>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -157,6 +158,7 @@ struct wx_ctx {
   DevBlock* dBlocks = nullptr;
   int32_t* dWork = nullptr;
   int32_t* dFlags = nullptr;
+  int32_t* dOps = nullptr;   // admesh: refine/coarsen operations, 9 slots each
   DevCtl* dCtl = nullptr;
   DevCtl* hCtl = nullptr;   // pinned mirror
   double* dCool = nullptr;  // COOL_TABLE [2][ncool]; METAL [ncool+1][nZ+1]; SCHURE [2][180]
@@ -604,7 +606,9 @@ int wx3d_config_defaults(wx_config* f) {
 const char* wx3d_error_string(int32_t code) {
   switch (code) {
     case WX_OK: return "ok";
+    case WX_ERR_ALREADY_MAX_LEV: return "block already at the finest level";
     case WX_ERR_INSUFICIENT_NBMAXPROC: return "not enough block slots";
+    case WX_ERR_REGISTER_FATHER: return "no free slot for a coarsened father block";
     case WX_ERR_TOO_MANY_LEVS: return "too many refinement levels";
     case WX_ERR_COOLING_LOAD_COEFS: return "bad cooling table";
     case WX_ERR_OUTPUT_FILE_OPEN: return "could not write an output file";
@@ -681,6 +685,7 @@ int wx3d_finalize(wx_ctx* c) {
   cudaFree(c->dBlocks); cudaFree(c->dWork); cudaFree(c->dFlags); cudaFree(c->dCtl); cudaFree(c->dCool);
   cudaFree(c->dTrust);
   cudaFree(c->dWind);
+  cudaFree(c->dOps);
   if (c->hCtl) cudaFreeHost(c->hCtl);
   for (int i = 0; i < 64; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -1489,6 +1494,236 @@ int wx3d_refine(wx_ctx* c, int32_t father, const int32_t* ch) {
   c->dt_valid = false;
   c->prestep = false;
   invalidate_graph(c);
+  return WX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// admesh (amr.f90:44-133) of one process.
+namespace {
+
+// localBlocks with the reference's registry operations (utils.f90:78-172):
+// find by bID, put into the first empty slot, pop (free) a block's slot;
+// hashed instead of the linear scans.
+struct SlotList {
+  std::vector<int32_t> lb;
+  std::unordered_map<long long, int> at;
+  std::set<int> empty;
+  explicit SlotList(const std::vector<int32_t>& l) : lb(l) {
+    for (int s = 0; s < (int)lb.size(); ++s) {
+      if (lb[s] == -1) empty.insert(s);
+      else at[lb[s]] = s;
+    }
+  }
+  int find(long long id) const {
+    auto it = at.find(id);
+    return it == at.end() ? -1 : it->second;
+  }
+  int put(long long id) {
+    if (empty.empty()) return -1;
+    const int s = *empty.begin();
+    empty.erase(empty.begin());
+    lb[s] = (int32_t)id;
+    at[id] = s;
+    return s;
+  }
+  void pop(long long id) {
+    auto it = at.find(id);
+    if (it == at.end()) return;
+    lb[it->second] = -1;
+    empty.insert(it->second);
+    at.erase(it);
+  }
+};
+
+long long tree_father(const Tree& T, long long id) {  // amr.f90:916-961
+  const int l = T.level(id);
+  if (l <= 1) return -1;
+  int x[3];
+  T.coords(id, l, x);
+  const int y[3] = {x[0] / 2, x[1] / 2, x[2] / 2};
+  return T.id(l - 1, y);
+}
+
+void tree_children(const Tree& T, long long id, long long out[8]) {  // amr.f90:882-909, x fastest
+  const int l = T.level(id);
+  int x[3];
+  T.coords(id, l, x);
+  for (int c = 0; c < 8; ++c) {
+    const int y[3] = {2 * x[0] + (c & 1), 2 * x[1] + ((c >> 1) & 1), 2 * x[2] + (c >> 2)};
+    out[c] = T.id(l + 1, y);
+  }
+}
+
+// Same-level region across face f (0..5 = left..top), -1 at the domain edge
+// (neighborLevel, amr.f90:439-523).
+long long tree_region(const Tree& T, long long id, int f) {
+  const int l = T.level(id);
+  int x[3];
+  T.coords(id, l, x);
+  const int ax = f / 2;
+  x[ax] += (f & 1) ? 1 : -1;
+  if (x[ax] < 0 || x[ax] >= T.nb[l][ax]) return -1;
+  return T.id(l, x);
+}
+
+// checkProximity (amr.f90:1109-1254) over the synchronised flags, level
+// finest down to 1, blocks in slot order; flags change as the sweep goes.
+void check_proximity(const Tree& T, const SlotList& L, std::vector<int>& flags, int finest) {
+  const std::vector<int32_t>& glob = L.lb;
+  for (int level = finest; level >= 1; --level)
+    for (int nb = 0; nb < (int)glob.size(); ++nb) {
+      const long long id = glob[nb];
+      if (id == -1 || T.level(id) != level) continue;
+      const int bflag = flags[nb];
+      if (bflag == WX_FLAG_REFINE) {
+        for (int f = 0; f < 6; ++f) {
+          const long long n = tree_region(T, id, f);
+          if (n < 0) continue;
+          const int s = L.find(n);
+          if (s >= 0) {  // same level: its coarsening is inhibited
+            if (flags[s] == WX_FLAG_COARSE) flags[s] = WX_FLAG_NONE;
+            continue;
+          }
+          const int sf = L.find(tree_father(T, n));
+          if (sf >= 0 && flags[sf] != WX_FLAG_REFINE) flags[sf] = WX_FLAG_REFINE;  // coarser: refined too
+        }
+      }
+      if (bflag == WX_FLAG_COARSE) {
+        bool inhibited = false;
+        for (int f = 0; f < 6 && !inhibited; ++f) {
+          const long long n = tree_region(T, id, f);
+          if (n < 0 || L.find(n) >= 0 || L.find(tree_father(T, n)) >= 0 || level >= T.maxlev) continue;
+          long long sib[8];  // finer neighbour: all eight children of the region
+          tree_children(T, n, sib);
+          for (int i = 0; i < 8; ++i) {
+            const int s = L.find(sib[i]);
+            if (s >= 0 && flags[s] != WX_FLAG_COARSE) {
+              flags[nb] = WX_FLAG_NONE;
+              inhibited = true;
+              break;
+            }
+          }
+        }
+      }
+    }
+}
+
+// Splits an operation list (9 slots each: father, then 8 children or
+// siblings) into runs in which no op writes a slot that an earlier op of the
+// same run reads; returns the run boundaries.
+std::vector<int> conflict_free_runs(const std::vector<int32_t>& ops, bool refine) {
+  std::vector<int> cuts{0};
+  std::unordered_map<int, int> reads;  // slot -> reading op, current run
+  const int n = (int)ops.size() / 9;
+  for (int o = 0; o < n; ++o) {
+    const int32_t* p = ops.data() + 9 * o;
+    bool clash = false;
+    if (refine) {
+      for (int c = 1; c <= 8 && !clash; ++c) clash = reads.count(p[c]) != 0;
+    } else {
+      clash = reads.count(p[0]) != 0;
+    }
+    if (clash) {
+      cuts.push_back(o);
+      reads.clear();
+    }
+    if (refine) reads[p[0]] = o;
+    else for (int c = 1; c <= 8; ++c) reads[p[c]] = o;
+  }
+  cuts.push_back(n);
+  return cuts;
+}
+
+}  // namespace
+
+int wx3d_admesh(wx_ctx* c, int32_t nbmax, int32_t* lb, int32_t* counts) {
+  if (!ready(c) || !lb) return WX_ERR_INVALID_ARG;
+  if (nbmax != c->max_blocks) return fail(c, WX_ERR_INVALID_ARG, "local_blocks must have max_blocks (%d) entries", c->max_blocks);
+  if (c->nhalo > 0) return fail(c, WX_ERR_UNSUPPORTED, "admesh of a partitioned mesh");
+  for (int s = 0; s < nbmax; ++s)
+    if (lb[s] != c->local[s]) return fail(c, WX_ERR_MESH, "slot %d: local_blocks differs from the mesh last set", s);
+  const Tree& T = c->tree;
+  // markByPhysical on the device; empty slots keep FLAG_NONE
+  std::vector<int32_t> mk(nbmax);
+  int rc = wx3d_mark(c, nbmax, mk.data());
+  if (rc) return rc;
+  std::vector<int> flags(nbmax, WX_FLAG_NONE);
+  for (int s = 0; s < nbmax; ++s)
+    if (lb[s] != -1) flags[s] = mk[s];
+  SlotList L(c->local);
+  check_proximity(T, L, flags, c->cfg.maxlev - 1);
+  // refineBlock for the marked blocks, in slot order of the list before it
+  const std::vector<int32_t> glob = c->local;
+  int nbLocal = (int)L.at.size();
+  std::vector<int32_t> rops, cops;
+  for (int nb = 0; nb < nbmax; ++nb) {
+    const long long id = glob[nb];
+    if (id == -1 || flags[nb] != WX_FLAG_REFINE) continue;
+    const int fi = L.find(id);
+    if (T.level(id) == c->cfg.maxlev) return fail(c, WX_ERR_ALREADY_MAX_LEV, "bID %lld is at the finest level", id);
+    if (nbLocal + 8 > nbmax)
+      return fail(c, WX_ERR_INSUFICIENT_NBMAXPROC, "refining bID %lld needs 8 slots; %d of %d are used", id, nbLocal, nbmax);
+    long long ch[8];
+    tree_children(T, id, ch);
+    rops.push_back(fi);
+    for (int k = 0; k < 8; ++k) rops.push_back(L.put(ch[k]));
+    L.pop(id);
+    nbLocal += 7;
+  }
+  // coarseBlocks: families in the order their first marked member appears
+  // (flags stay indexed by the slots before refinement; a new child only
+  // takes an empty or a refined father's slot, never a COARSE one)
+  std::vector<long long> fam;
+  std::unordered_map<long long, int> count;
+  for (int nb = 0; nb < nbmax; ++nb) {
+    const long long id = L.lb[nb];
+    if (id == -1 || flags[nb] != WX_FLAG_COARSE) continue;
+    long long sib[8];
+    tree_children(T, tree_father(T, id), sib);
+    if (count[sib[0]]++ == 0) fam.push_back(sib[0]);
+  }
+  int ncoarse = 0;
+  for (long long e : fam) {
+    if (count[e] != 8) continue;
+    const long long fid = tree_father(T, e);
+    long long sib[8];
+    tree_children(T, fid, sib);
+    const int fslot = L.put(fid);
+    if (fslot < 0) return fail(c, WX_ERR_REGISTER_FATHER, "no free slot for father bID %lld", fid);
+    cops.push_back(fslot);
+    for (int k = 0; k < 8; ++k) {
+      cops.push_back(L.find(sib[k]));
+      L.pop(sib[k]);
+    }
+    ++ncoarse;
+  }
+  // data: refinements, then coarsenings, in conflict-free runs
+  if (!rops.empty() || !cops.empty()) {
+    if (!c->dOps) WX_CUDA(cudaMalloc(&c->dOps, sizeof(int32_t) * 9 * (size_t)c->max_blocks));
+    for (int pass = 0; pass < 2; ++pass) {
+      const std::vector<int32_t>& ops = pass == 0 ? rops : cops;
+      if (ops.empty()) continue;
+      WX_CUDA(cudaMemcpyAsync(c->dOps, ops.data(), 4 * ops.size(), cudaMemcpyHostToDevice, c->stream));
+      const std::vector<int> cut = conflict_free_runs(ops, pass == 0);
+      for (size_t r = 0; r + 1 < cut.size(); ++r)
+        for (int o = cut[r]; o < cut[r + 1]; o += 8000) {
+          const int n = std::min(8000, cut[r + 1] - o);
+          if (pass == 0) refine_batch_kernel<<<dim3(16, 8 * n), 256, 0, c->stream>>>(c->dU, c->neq, c->dOps + 9 * o);
+          else coarsen_batch_kernel<<<dim3(4, 8 * n), 256, 0, c->stream>>>(c->dU, c->neq, c->dOps + 9 * o);
+          WX_LAUNCHED();
+        }
+      WX_CUDA(cudaStreamSynchronize(c->stream));  // dOps is refilled by the next pass
+    }
+  }
+  c->dt_valid = false;
+  c->prestep = false;
+  invalidate_graph(c);
+  if ((rc = wx3d_set_mesh(c, nbmax, L.lb.data()))) return rc;
+  std::copy(L.lb.begin(), L.lb.end(), lb);
+  if (counts) {
+    counts[0] = (int32_t)(rops.size() / 9);
+    counts[1] = ncoarse;
+  }
   return WX_OK;
 }
 

@@ -265,6 +265,38 @@ __global__ void coarsen_kernel(double* __restrict__ u, int neq, int father, Slot
   }
 }
 
+// Batched forms for admesh: op = [father, child0..child7] (9 slots), one
+// CTA row per (op, child) or (op, sibling).  No slot is written by one op of
+// a batch and read by another: the host cuts batches where a freed slot is
+// taken again.
+__global__ void refine_batch_kernel(double* __restrict__ u, int neq, const int32_t* __restrict__ ops) {
+  const int op = blockIdx.y >> 3, cc = blockIdx.y & 7;
+  const int father = ops[9 * op], child = ops[9 * op + 1 + cc];
+  const int sx = cc & 1, sy = (cc >> 1) & 1, sz = (cc >> 2) & 1;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < BCELLS * neq; c += gridDim.x * blockDim.x) {
+    const int e = c / BCELLS, r = c % BCELLS;
+    const int i = (r & 15) + 1, j = ((r >> 4) & 15) + 1, k = (r >> 8) + 1;
+    const int ip = 8 * sx + (i + 1) / 2, jp = 8 * sy + (j + 1) / 2, kp = 8 * sz + (k + 1) / 2;
+    u[cell_off(child, neq, e, i, j, k)] = u[cell_off(father, neq, e, ip, jp, kp)];
+  }
+}
+
+__global__ void coarsen_batch_kernel(double* __restrict__ u, int neq, const int32_t* __restrict__ ops) {
+  const int op = blockIdx.y >> 3, sib = blockIdx.y & 7;
+  const int father = ops[9 * op], child = ops[9 * op + 1 + sib];
+  const int sx = sib & 1, sy = (sib >> 1) & 1, sz = (sib >> 2) & 1;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < 512 * neq; c += gridDim.x * blockDim.x) {
+    const int e = c / 512, r = c % 512;
+    const int i = (r & 7) + 1, j = ((r >> 3) & 7) + 1, k = (r >> 6) + 1;
+    const int i1 = 2 * i - 1, j1 = 2 * j - 1, k1 = 2 * k - 1;
+    double s = 0.0;
+    for (int kk = k1; kk <= k1 + 1; ++kk)
+      for (int jj = j1; jj <= j1 + 1; ++jj)
+        for (int ii = i1; ii <= i1 + 1; ++ii) s += u[cell_off(child, neq, e, ii, jj, kk)];
+    u[cell_off(father, neq, e, i + 8 * sx, j + 8 * sy, k + 8 * sz)] = s / 8.0;
+  }
+}
+
 // Primitive variables of the physical cells (calcPrimsBlock CELLS_PHYS).
 template <int NEQ, bool MHD>
 __global__ void prims_kernel(const double* __restrict__ u, double* __restrict__ prim, const int32_t* __restrict__ work,

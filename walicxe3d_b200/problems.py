@@ -160,6 +160,31 @@ def orszag_tang_3d(nroot: int = 2, flux_cd: bool = True, solver=C.SOLVER_HLLD, s
     return _finish("orszag-tang-3d", cfg, tree, prim_fn, steps)
 
 
+def amr_pulse(nroot: int = 2, maxlev: int = 3, centre=(0.15, 0.15, 0.15), width: float = 0.03,
+              amplitude: float = 10.0, steps: int = 20) -> Problem:
+    """Live-mesh test: a Gaussian pressure and density pulse in one corner of
+    a uniform medium at rest (rho = p = 1), on nroot^3 root blocks all
+    refined once (level 2).  The first admesh coarsens the quiet families and
+    refines the blocks around the pulse; as the pulse spreads, refinement
+    follows it.  HLLC + minmod, CFL 0.4, eta 5e-3, free-flow boundaries."""
+    cfg = Config(solver_type=C.SOLVER_HLLC, limiter_type=C.LIMITER_MINMOD, nbroot=(nroot,) * 3, maxlev=maxlev,
+                 gamma=5.0 / 3.0, cfl=0.4, visc_eta=5.0e-3)
+    tree = BlockTree(cfg.nbroot, maxlev).roots()
+    for b in sorted(tree.leaves):
+        tree.refine(b)
+    c = np.array(centre)
+
+    def prim_fn(xyz):
+        r2 = ((xyz - c[None, :, None, None, None]) ** 2).sum(axis=1)
+        g = amplitude * np.exp(-r2 / width ** 2)
+        prim = np.zeros((xyz.shape[0], cfg.neqtot) + xyz.shape[2:])
+        prim[:, 0] = 1.0 + 0.5 * g
+        prim[:, 4] = 1.0 + g
+        return prim
+
+    return _finish("amr-pulse", cfg, tree, prim_fn, steps)
+
+
 def smooth_pulse(nroot: int = 2, amplitude: float = 0.2, width: float = 0.15, solver=C.SOLVER_HLLC,
                  limiter=C.LIMITER_MINMOD) -> Problem:
     """Smooth Gaussian density/pressure pulse at rest in a uniform medium

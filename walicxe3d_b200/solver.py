@@ -82,6 +82,21 @@ class Walicxe3D:
         lb, p = _i32(local_blocks)
         self._chk(self.lib.wx3d_set_mesh(self.ctx, len(lb), p), "wx3d_set_mesh")
         self.nslots = len(lb)
+        self.local_blocks = np.full(self.max_blocks, -1, np.int32)
+        self.local_blocks[:len(lb)] = lb
+
+    def admesh(self):
+        """admesh (amr.f90:44-133): mark, proximity rule, refine and coarsen
+        in the reference's slot order; updates ``local_blocks`` (all
+        max_blocks slots, -1 = empty) and returns (blocks refined, families
+        coarsened)."""
+        lb = np.ascontiguousarray(self.local_blocks, dtype=np.int32)
+        n = np.zeros(2, np.int32)
+        self._chk(self.lib.wx3d_admesh(self.ctx, self.max_blocks, lb.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                       n.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))), "wx3d_admesh")
+        self.local_blocks = lb
+        self.nslots = self.max_blocks
+        return int(n[0]), int(n[1])
 
     def set_zsplit(self, z: int):
         self._chk(self.lib.wx3d_set_zsplit(self.ctx, int(z)), "wx3d_set_zsplit")
