@@ -197,6 +197,53 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def live_mesh_leg(prob, args, stream):
+    """Throughput with a live mesh (main.f90:79-103 with admesh after every
+    step): a fresh context with room for 3x the snapshot's blocks runs W
+    warm-up and K timed iterations of wx3d_step followed by wx3d_admesh,
+    timed with CUDA events on the library's stream around the K iterations.
+    The cells of each step are the leaves of the mesh that step ran on."""
+    import torch
+    from walicxe3d_b200._lib import WxError
+    from walicxe3d_b200.solver import from_problem
+    w = from_problem(prob, extra_slots=2 * prob.nblocks)
+    w.set_stream(stream.cuda_stream)
+    nblocks = prob.nblocks
+    out = {"unit": "Mcell-updates/s", "steps": args.steps, "blocks_start": nblocks}
+    try:
+        for _ in range(args.warmup):
+            w.step()
+            w.admesh()
+        nblocks = int((w.local_blocks != -1).sum())
+        out["blocks_after_warmup"] = nblocks
+        torch.cuda.synchronize()
+        cells, ref, crs, t_ad = 0, 0, 0, 0.0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            cells += nblocks * 4096
+            w.step()
+            t0 = time.perf_counter()
+            r, c = w.admesh()
+            t_ad += time.perf_counter() - t0
+            ref, crs = ref + r, crs + c
+            nblocks = int((w.local_blocks != -1).sum())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out.update({"value": cells / (ms / 1e3) / 1e6, "ms_per_step": ms / args.steps,
+                    "admesh_ms_per_call": 1e3 * t_ad / args.steps, "blocks_end": nblocks,
+                    "refined": ref, "coarsened_families": crs,
+                    "note": "each step: wx3d_step (synchronous) then wx3d_admesh (device marking, proximity rule "
+                            "and slot registry on the host, batched refine/coarsen copies, neighbour-table "
+                            "rebuild)"})
+    except WxError as e:
+        out["error"] = str(e)
+    finally:
+        w.close()
+    return out
+
+
 def run_partition(args, prob, rank, world, dist):
     """One mesh shared by the ranks (walicxe3d_b200.partition): each owns a
     Morton share plus halo copies, exchanged over NCCL between the stages;
@@ -260,6 +307,7 @@ def main():
     ap.add_argument("--workload", default="blast-amr", choices=sorted(WORKLOADS))
     ap.add_argument("--zsplit", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-live-mesh", action="store_true", help="skip the live-mesh (admesh every step) leg")
     ap.add_argument("--partition", action="store_true",
                     help="strong scaling: the ranks share one mesh (halo exchange over NCCL) instead of replicas")
     ap.add_argument("--surrogate", action="store_true",
@@ -392,6 +440,11 @@ def main():
     e2e_value = prob.cells * args.steps * world / e2e_s / 1e6
     state_bytes = prob.U.nbytes
 
+    w.close()
+    live = None
+    if rank == 0 and not args.no_live_mesh and not args.surrogate and prob.tree.maxlev > 1 and not prob.winds:
+        live = live_mesh_leg(prob, args, stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, n, secs = cpu_time_oracle(prob, 1000, float(os.environ.get("WX3D_CPU_BUDGET_S", "20")), os.cpu_count() or 1)
@@ -426,6 +479,7 @@ def main():
                     "note": "timed: upload of the state from pinned host memory, K wx3d_step calls (each "
                             "returns time/dt/status to the host), download of the final state"},
             "gpu_launches": launches,
+            "live_mesh": live,
             "surrogate": ({"attached": True, "surrogate_cells": sur_cells, "fallback_cells": fb_cells,
                            "share": sur_cells / max(1, sur_cells + fb_cells)} if args.surrogate else None),
             "clocks": clocks,
@@ -433,7 +487,6 @@ def main():
             "final_state": {"time": st.time, "dt": st.dt, "it": st.it},
         }
         print(json.dumps(line), flush=True)
-    w.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

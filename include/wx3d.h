@@ -326,7 +326,9 @@ int wx3d_coarsen(wx_ctx* ctx, const int32_t* child_slots8, int32_t father_slot);
  * process loadBalance moves no block, so the slot order is the reference's.
  * local_blocks (nbmax = the context's max_blocks entries, -1 = empty) must
  * hold the list last passed to wx3d_set_mesh, padded with -1; on return it
- * holds the new list and the device neighbour table is rebuilt from it.
+ * holds the new list.  When a block changed, the device neighbour table is
+ * rebuilt from it (the context's z-slab split is kept); otherwise nothing
+ * but the marking runs.
  * counts2 (may be NULL): blocks refined, families coarsened.  Capacity
  * errors (WX_ERR_INSUFICIENT_NBMAXPROC, WX_ERR_REGISTER_FATHER) are found
  * before any data moves and leave the mesh and the state unchanged. */

@@ -11,7 +11,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
-#include <set>
+#include <functional>
+#include <queue>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -135,6 +136,65 @@ struct Tree {
   long long id(int l, const int x[3]) const {
     return minID[l] + x[0] + (long long)nb[l][0] * (x[1] + (long long)nb[l][1] * x[2]);
   }
+};
+
+// bID -> slot for the neighbour-table build and admesh's slot registry: open
+// addressing with linear probing in a power-of-two table at most half full,
+// deletion by backward shift (no tombstones), so every lookup is a short
+// scan of one cache line or two.
+class SlotMap {
+ public:
+  explicit SlotMap(size_t n) {
+    int bits = 4;
+    while ((size_t(1) << bits) < 2 * n + 16) ++bits;
+    shift_ = 64 - bits;
+    mask_ = (size_t(1) << bits) - 1;
+    key_.assign(mask_ + 1, -1);
+    val_.assign(mask_ + 1, -1);
+  }
+  int find(long long k) const {
+    for (size_t i = home(k);; i = (i + 1) & mask_) {
+      if (key_[i] == k) return val_[i];
+      if (key_[i] == -1) return -1;
+    }
+  }
+  bool insert(long long k, int v) {  // false if k is present
+    for (size_t i = home(k);; i = (i + 1) & mask_) {
+      if (key_[i] == k) return false;
+      if (key_[i] == -1) {
+        key_[i] = k;
+        val_[i] = v;
+        ++n_;
+        return true;
+      }
+    }
+  }
+  void erase(long long k) {
+    size_t i = home(k);
+    while (key_[i] != k) {
+      if (key_[i] == -1) return;
+      i = (i + 1) & mask_;
+    }
+    for (size_t j = i;;) {  // shift back the entries of the run that may fill the hole
+      j = (j + 1) & mask_;
+      if (key_[j] == -1) break;
+      if (((j - home(key_[j])) & mask_) >= ((j - i) & mask_)) {
+        key_[i] = key_[j];
+        val_[i] = val_[j];
+        i = j;
+      }
+    }
+    key_[i] = -1;
+    --n_;
+  }
+  size_t size() const { return n_; }
+
+ private:
+  size_t home(long long k) const { return (size_t)(((unsigned long long)k * 0x9E3779B97F4A7C15ull) >> shift_); }
+  std::vector<long long> key_;
+  std::vector<int> val_;
+  size_t mask_ = 0, n_ = 0;
+  int shift_ = 60;
 };
 
 }  // namespace
@@ -719,19 +779,21 @@ int wx3d_set_mesh_halo(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nha
   if (nhalo > 0 && !c->hwind.empty()) return fail(c, WX_ERR_UNSUPPORTED, "wind sources in a partitioned run");
   if (nslots > c->max_blocks) return fail(c, WX_ERR_INSUFICIENT_NBMAXPROC, "%d slots > max_blocks %d", nslots, c->max_blocks);
   const Tree& T = c->tree;
-  std::unordered_map<long long, int> slot;
-  slot.reserve((size_t)nslots * 2);
+  SlotMap slot((size_t)nslots);
   for (int s = 0; s < nslots; ++s) {
     if (lb[s] == -1) continue;
     if (T.level(lb[s]) < 1) return fail(c, WX_ERR_MESH, "slot %d: bID %d outside the tree", s, lb[s]);
-    if (!slot.emplace(lb[s], s).second) return fail(c, WX_ERR_MESH, "bID %d registered twice", lb[s]);
+    if (!slot.insert(lb[s], s)) return fail(c, WX_ERR_MESH, "bID %d registered twice", lb[s]);
   }
+  // the table entry of every slot, independent per slot (over the host
+  // cores); a face without a valid neighbour is reported as 1 + 2*face +
+  // (0: no active neighbour at the finest level, 1: not one level apart)
   std::vector<DevBlock> hb(c->max_blocks);
-  std::vector<int32_t> work;
-  for (int s = 0; s < nslots; ++s) {
+  std::vector<int> face_err(nslots, 0);
+  auto entry = [&](int s) -> int {
     DevBlock b{};
     const long long id = lb[s];
-    if (id == -1) { hb[s] = b; continue; }
+    if (id == -1) { hb[s] = b; return 0; }
     const int l = T.level(id);
     int x[3];
     T.coords(id, l, x);
@@ -756,18 +818,18 @@ int wx3d_set_mesh_halo(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nha
         continue;
       }
       const long long nID = T.id(l, y);
-      auto it = slot.find(nID);
-      if (it != slot.end()) { b.ftype[f] = WX_NEIGH_SAME; b.fnb[f][0] = it->second; continue; }
+      const int sn = slot.find(nID);
+      if (sn >= 0) { b.ftype[f] = WX_NEIGH_SAME; b.fnb[f][0] = sn; continue; }
       if (l > 1) {
         int z[3] = {y[0] / 2, y[1] / 2, y[2] / 2};
-        auto ft = slot.find(T.id(l - 1, z));
-        if (ft != slot.end()) { b.ftype[f] = WX_NEIGH_COARSER; b.fnb[f][0] = ft->second; continue; }
+        const int sf = slot.find(T.id(l - 1, z));
+        if (sf >= 0) { b.ftype[f] = WX_NEIGH_COARSER; b.fnb[f][0] = sf; continue; }
       }
       // finer: the four children of nID adjacent to this face, transverse
       // axes in x<y<z order (amr.f90:590-628)
       if (l >= T.maxlev) {
         if (is_halo[s]) { b.ftype[f] = 0; continue; }   // outside the local set
-        return fail(c, WX_ERR_MESH, "bID %lld face %d: no active neighbour", id, f + 1);
+        return 1 + 2 * f;
       }
       const int t1 = ax == 0 ? 1 : 0, t2 = ax == 2 ? 1 : 2;
       b.ftype[f] = WX_NEIGH_FINER;
@@ -776,16 +838,28 @@ int wx3d_set_mesh_halo(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nha
         ch[ax] = 2 * y[ax] + (side ? 0 : 1);
         ch[t1] = 2 * y[t1] + (q & 1);
         ch[t2] = 2 * y[t2] + (q >> 1);
-        auto ct = slot.find(T.id(l + 1, ch));
-        if (ct == slot.end()) {
+        const int sc = slot.find(T.id(l + 1, ch));
+        if (sc < 0) {
           if (is_halo[s]) { b.ftype[f] = 0; break; }
-          return fail(c, WX_ERR_MESH, "bID %lld face %d: neighbour region is neither same, coarser nor finer by one", id, f + 1);
+          return 2 + 2 * f;
         }
-        b.fnb[f][q] = ct->second;
+        b.fnb[f][q] = sc;
       }
     }
     hb[s] = b;
-    if (!is_halo[s]) work.push_back(s);
+    return 0;
+  };
+#pragma omp parallel for schedule(dynamic, 512) if (nslots > 4096)
+  for (int s = 0; s < nslots; ++s) face_err[s] = entry(s);
+  std::vector<int32_t> work;
+  work.reserve(nslots);
+  for (int s = 0; s < nslots; ++s) {
+    if (face_err[s]) {
+      const int f = (face_err[s] - 1) / 2;
+      if ((face_err[s] - 1) % 2 == 0) return fail(c, WX_ERR_MESH, "bID %d face %d: no active neighbour", lb[s], f + 1);
+      return fail(c, WX_ERR_MESH, "bID %d face %d: neighbour region is neither same, coarser nor finer by one", lb[s], f + 1);
+    }
+    if (lb[s] != -1 && !is_halo[s]) work.push_back(s);
   }
   c->local.assign(c->max_blocks, -1);
   std::copy(lb, lb + nslots, c->local.begin());
@@ -794,12 +868,12 @@ int wx3d_set_mesh_halo(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nha
   if (!flag_wind_blocks(c, hb, &bad))
     return fail(c, WX_ERR_UNSUPPORTED, "slot %d: a wind sphere reaches the ghost layer of a coarse/fine face; "
                 "refine the zone around the source (refineZone) further", bad);
-  c->hblocks = hb;
-  c->work = work;
-  c->nwork = (int)work.size();
-  WX_CUDA(cudaMemcpyAsync(c->dBlocks, hb.data(), sizeof(DevBlock) * c->max_blocks, cudaMemcpyHostToDevice, c->stream));
-  if (!work.empty())
-    WX_CUDA(cudaMemcpyAsync(c->dWork, work.data(), 4 * work.size(), cudaMemcpyHostToDevice, c->stream));
+  c->hblocks = std::move(hb);
+  c->work = std::move(work);
+  c->nwork = (int)c->work.size();
+  WX_CUDA(cudaMemcpyAsync(c->dBlocks, c->hblocks.data(), sizeof(DevBlock) * c->max_blocks, cudaMemcpyHostToDevice, c->stream));
+  if (!c->work.empty())
+    WX_CUDA(cudaMemcpyAsync(c->dWork, c->work.data(), 4 * c->work.size(), cudaMemcpyHostToDevice, c->stream));
   WX_CUDA(cudaStreamSynchronize(c->stream));
   // small meshes split every block into z-slabs so all SMs get work
   c->zsplit = 1;
@@ -1503,35 +1577,34 @@ namespace {
 
 // localBlocks with the reference's registry operations (utils.f90:78-172):
 // find by bID, put into the first empty slot, pop (free) a block's slot;
-// hashed instead of the linear scans.
+// a hash table and a min-heap of the empty slots instead of linear scans.
 struct SlotList {
   std::vector<int32_t> lb;
-  std::unordered_map<long long, int> at;
-  std::set<int> empty;
-  explicit SlotList(const std::vector<int32_t>& l) : lb(l) {
+  SlotMap at;
+  std::priority_queue<int, std::vector<int>, std::greater<int>> empty;
+  explicit SlotList(const std::vector<int32_t>& l) : lb(l), at(l.size()) {
+    std::vector<int> e;
     for (int s = 0; s < (int)lb.size(); ++s) {
-      if (lb[s] == -1) empty.insert(s);
-      else at[lb[s]] = s;
+      if (lb[s] == -1) e.push_back(s);
+      else at.insert(lb[s], s);
     }
+    empty = decltype(empty)(std::greater<int>(), std::move(e));
   }
-  int find(long long id) const {
-    auto it = at.find(id);
-    return it == at.end() ? -1 : it->second;
-  }
+  int find(long long id) const { return at.find(id); }
   int put(long long id) {
     if (empty.empty()) return -1;
-    const int s = *empty.begin();
-    empty.erase(empty.begin());
+    const int s = empty.top();
+    empty.pop();
     lb[s] = (int32_t)id;
-    at[id] = s;
+    at.insert(id, s);
     return s;
   }
   void pop(long long id) {
-    auto it = at.find(id);
-    if (it == at.end()) return;
-    lb[it->second] = -1;
-    empty.insert(it->second);
-    at.erase(it);
+    const int s = at.find(id);
+    if (s < 0) return;
+    lb[s] = -1;
+    empty.push(s);
+    at.erase(id);
   }
 };
 
@@ -1570,10 +1643,12 @@ long long tree_region(const Tree& T, long long id, int f) {
 // finest down to 1, blocks in slot order; flags change as the sweep goes.
 void check_proximity(const Tree& T, const SlotList& L, std::vector<int>& flags, int finest) {
   const std::vector<int32_t>& glob = L.lb;
+  std::vector<std::vector<int>> by_level(T.maxlev + 1);  // occupied slots per level, ascending
+  for (int nb = 0; nb < (int)glob.size(); ++nb)
+    if (glob[nb] != -1) by_level[T.level(glob[nb])].push_back(nb);
   for (int level = finest; level >= 1; --level)
-    for (int nb = 0; nb < (int)glob.size(); ++nb) {
+    for (const int nb : by_level[level]) {
       const long long id = glob[nb];
-      if (id == -1 || T.level(id) != level) continue;
       const int bflag = flags[nb];
       if (bflag == WX_FLAG_REFINE) {
         for (int f = 0; f < 6; ++f) {
@@ -1697,8 +1772,13 @@ int wx3d_admesh(wx_ctx* c, int32_t nbmax, int32_t* lb, int32_t* counts) {
     }
     ++ncoarse;
   }
+  if (counts) {
+    counts[0] = (int32_t)(rops.size() / 9);
+    counts[1] = ncoarse;
+  }
+  if (rops.empty() && cops.empty()) return WX_OK;  // the mesh and the state stay as they are
   // data: refinements, then coarsenings, in conflict-free runs
-  if (!rops.empty() || !cops.empty()) {
+  {
     if (!c->dOps) WX_CUDA(cudaMalloc(&c->dOps, sizeof(int32_t) * 9 * (size_t)c->max_blocks));
     for (int pass = 0; pass < 2; ++pass) {
       const std::vector<int32_t>& ops = pass == 0 ? rops : cops;
@@ -1715,15 +1795,10 @@ int wx3d_admesh(wx_ctx* c, int32_t nbmax, int32_t* lb, int32_t* counts) {
       WX_CUDA(cudaStreamSynchronize(c->stream));  // dOps is refilled by the next pass
     }
   }
-  c->dt_valid = false;
-  c->prestep = false;
-  invalidate_graph(c);
+  const int zsplit = c->zsplit;  // the launch shape chosen for the context stays
   if ((rc = wx3d_set_mesh(c, nbmax, L.lb.data()))) return rc;
+  c->zsplit = zsplit;
   std::copy(L.lb.begin(), L.lb.end(), lb);
-  if (counts) {
-    counts[0] = (int32_t)(rops.size() / 9);
-    counts[1] = ncoarse;
-  }
   return WX_OK;
 }
 

@@ -165,50 +165,63 @@ __global__ void __launch_bounds__(256) mark_kernel(MarkParams P) {
   __shared__ double pp[3][18 * 18], pr[3][18 * 18];  // pressure and density, planes k-1..k+1
   __shared__ int first_refine;                        // first cell (loop order) reaching refineThres
   __shared__ double bmax;
+  __shared__ __align__(16) DevBlock B;                // the block's neighbour-table entry
   const int t = threadIdx.x;
   const int i = (t & 15) + 1, j = (t >> 4) + 1;
   auto q = [](int ii, int jj) { return ii + 18 * jj; };
   for (int w = blockIdx.x; w < P.nwork; w += gridDim.x) {
     const int slot = P.work[w];
-    const DevBlock& B = P.blocks[slot];
     __syncthreads();
+    if (t < (int)(sizeof(DevBlock) / 4)) reinterpret_cast<int*>(&B)[t] = reinterpret_cast<const int*>(P.blocks + slot)[t];
     if (t == 0) { first_refine = 0x7fffffff; bmax = 0.0; }
+    __syncthreads();
     double lmax = 0.0;
     int lfirst = 0x7fffffff;
-    // plane kk into ring slot kk%3 (kk = 0..17)
-    auto load = [&](int kk) {
+    // plane kk (0..17) is fetched into registers one plane ahead, then
+    // converted into ring slot kk%3, so its loads overlap the gradients of
+    // the plane before
+    const int side = t >> 4, r = (t & 15) + 1;
+    const int gi = side == 0 ? 0 : (side == 1 ? NC + 1 : r);
+    const int gj = side == 2 ? 0 : (side == 3 ? NC + 1 : r);
+    double ua[NEQ], ug[NEQ];
+    auto fetch = [&](int kk) {
+      get_cell<NEQ>((kk >= 1 && kk <= NC) ? P.u : P.g, B, slot, i, j, kk, ua);
+      if (kk >= 1 && kk <= NC && t < 64) gather_ghost<NEQ>(P.g, B, slot, gi, gj, kk, ug);
+    };
+    auto commit = [&](int kk) {
       const int s = kk % 3;
-      double u[NEQ], p[NEQ];
-      get_cell<NEQ>((kk >= 1 && kk <= NC) ? P.u : P.g, B, slot, i, j, kk, u);
-      flow2prim<NEQ, MHD>(u, p, P.ph.cv);
+      double p[NEQ];
+      flow2prim<NEQ, MHD>(ua, p, P.ph.cv);
       pp[s][q(i, j)] = p[4];
       pr[s][q(i, j)] = p[0];
       if (kk >= 1 && kk <= NC && t < 64) {
-        const int side = t >> 4, r = (t & 15) + 1;
-        int gi, gj;
-        if (side == 0) { gi = 0; gj = r; } else if (side == 1) { gi = NC + 1; gj = r; }
-        else if (side == 2) { gi = r; gj = 0; } else { gi = r; gj = NC + 1; }
-        gather_ghost<NEQ>(P.g, B, slot, gi, gj, kk, u);
-        flow2prim<NEQ, MHD>(u, p, P.ph.cv);
+        flow2prim<NEQ, MHD>(ug, p, P.ph.cv);
         pp[s][q(gi, gj)] = p[4];
         pr[s][q(gi, gj)] = p[0];
       }
     };
-    load(0);
-    load(1);
+    fetch(0);
+    commit(0);
+    fetch(1);
+    commit(1);
+    fetch(2);
     for (int k = 1; k <= NC; ++k) {
-      load(k + 1);
+      commit(k + 1);
+      if (k + 2 <= NC + 1) fetch(k + 2);
       __syncthreads();
       const int sm = (k - 1) % 3, sc = k % 3, sp = (k + 1) % 3;
       const double dx2 = 2 * B.dx;
 #pragma unroll
       for (int v = 0; v < 2; ++v) {
         double (*a)[18 * 18] = v == 0 ? pp : pr;
+        // max over the axes of |delta|/c/dx2: correctly rounded division by
+        // the same positive c and dx2 is monotonic, so dividing the largest
+        // |delta| gives the reference's max of the three quotients bit for bit
         const double c = a[sc][q(i, j)];
-        const double gx = fabs(a[sc][q(i + 1, j)] - a[sc][q(i - 1, j)]) / c / dx2;
-        const double gy = fabs(a[sc][q(i, j + 1)] - a[sc][q(i, j - 1)]) / c / dx2;
-        const double gz = fabs(a[sp][q(i, j)] - a[sm][q(i, j)]) / c / dx2;
-        const double gr = dmax(dmax(gx, gy), gz);
+        const double dx_ = fabs(a[sc][q(i + 1, j)] - a[sc][q(i - 1, j)]);
+        const double dy_ = fabs(a[sc][q(i, j + 1)] - a[sc][q(i, j - 1)]);
+        const double dz_ = fabs(a[sp][q(i, j)] - a[sm][q(i, j)]);
+        const double gr = dmax(dmax(dx_, dy_), dz_) / c / dx2;
         lmax = dmax(lmax, gr);
         // reference loop order: i outer, j, k inner; pressure before density
         const int order = (((i - 1) * NC + (j - 1)) * NC + (k - 1)) * 2 + v;
