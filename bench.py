@@ -412,6 +412,29 @@ def main():
                 "peak_source": "measured in this run (wx3d_measure_fp64_peak, DFMA chains)",
                 "note": "the stage kernels are bound by FP64 issue, not by HBM"}
 
+    # --- the plain GPU path: the same kernels, one synchronous wx3d_step per
+    # step (host round trip each step), default launch shape, no graph ---
+    plain = None
+    if rank == 0:
+        from walicxe3d_b200.solver import from_problem as _fp
+        wp = _fp(prob)
+        wp.set_stream(stream.cuda_stream)
+        for _ in range(args.warmup):
+            wp.step()
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(args.steps):
+            wp.step()
+        p1.record(stream)
+        torch.cuda.synchronize()
+        pms = p0.elapsed_time(p1)
+        wp.close()
+        plain = {"value": prob.cells * args.steps / (pms / 1e3) / 1e6, "unit": "Mcell-updates/s",
+                 "ms_per_step": pms / args.steps, "batched_gain": value / world / (prob.cells * args.steps / (pms / 1e3) / 1e6),
+                 "note": "wx3d_step per step (returns time/dt/status to the host), launch shape from the mesh "
+                         "size alone, no CUDA graph; batched = the timed wx3d_run graph replay with the autotuned shape"}
+
     # --- end to end through the C-ABI with host buffers ---
     U_host = torch.from_numpy(prob.U).pin_memory()
     U_out = torch.empty_like(U_host).pin_memory()
@@ -480,6 +503,7 @@ def main():
                             "returns time/dt/status to the host), download of the final state"},
             "gpu_launches": launches,
             "live_mesh": live,
+            "plain_steps": plain,
             "surrogate": ({"attached": True, "surrogate_cells": sur_cells, "fallback_cells": fb_cells,
                            "share": sur_cells / max(1, sur_cells + fb_cells)} if args.surrogate else None),
             "clocks": clocks,

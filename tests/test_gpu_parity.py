@@ -510,6 +510,15 @@ def test_field_cd_matches_oracle(shape, solver, ncpu):
     check(o, g, prob)
 
 
+def test_field_cd_on_a_refined_mesh_matches_oracle(ncpu):
+    """Field-CD on a two-level mesh: the electric field of the ghost cells
+    comes through coarse/fine faces (injected or averaged primitives)."""
+    prob = problems.orszag_tang_3d(nroot=4, maxlev=2)
+    assert {prob.tree.level(int(b)) for b in prob.local_blocks} == {1, 2}
+    o, g = run_both(prob, 10, ncpu)
+    check(o, g, prob)
+
+
 def test_field_cd_keeps_the_central_divergence_on_the_gpu():
     """4^3 blocks of the 3-D Orszag-Tang vortex, 20 steps through the CUDA
     graph: the central-difference divergence of B stays at its initial value

@@ -127,7 +127,8 @@ def brio_wu(nblocks_x: int = 16, steps: int = 0) -> Problem:
     return _finish("brio-wu", cfg, tree, prim_fn, steps or 200)
 
 
-def orszag_tang_3d(nroot: int = 2, flux_cd: bool = True, solver=C.SOLVER_HLLD, steps: int = 20) -> Problem:
+def orszag_tang_3d(nroot: int = 2, flux_cd: bool = True, solver=C.SOLVER_HLLD, steps: int = 20,
+                   maxlev: int = 1) -> Problem:
     """Orszag-Tang vortex (the reference's orzag-tang example; its problem
     file is not in the tree) extended to 3-D: unit box of nroot^3 root
     blocks, gamma=5/3, rho=25/(36 pi), p=5/(12 pi),
@@ -136,11 +137,15 @@ def orszag_tang_3d(nroot: int = 2, flux_cd: bool = True, solver=C.SOLVER_HLLD, s
     (B_z depends on z, so the field starts with a non-zero divergence),
     minmod, CFL 0.4, no viscosity, free-flow boundaries.  With flux_cd the
     magnetic field takes the field-CD update (brio-wu/flux_cd.f90:52-86)
-    instead of the 8-wave source."""
+    instead of the 8-wave source.  With maxlev > 1 the blocks within 0.2 of
+    the box centre are refined to maxlev (face-balanced), so the electric
+    field also crosses coarse/fine faces."""
     cfg = Config(bfield=True, mhd=True, solver_type=solver, limiter_type=C.LIMITER_MINMOD,
-                 eight_wave=not flux_cd, enable_flux_cd=flux_cd, nbroot=(nroot,) * 3, maxlev=1,
+                 eight_wave=not flux_cd, enable_flux_cd=flux_cd, nbroot=(nroot,) * 3, maxlev=maxlev,
                  gamma=5.0 / 3.0, cfl=0.4, visc_eta=0.0)
-    tree = BlockTree(cfg.nbroot, 1).roots()
+    tree = BlockTree(cfg.nbroot, maxlev).roots()
+    if maxlev > 1:
+        tree.refine_where(lambda lev, lo, hi: np.sqrt(((np.clip(0.5, lo, hi) - 0.5) ** 2).sum()) < 0.2, maxlev)
     b0 = 1.0 / np.sqrt(4.0 * np.pi)
 
     def prim_fn(xyz):
