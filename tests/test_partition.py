@@ -118,3 +118,23 @@ def test_partitioned_step_equals_single_context(name, nranks):
     for r in group.ranks:
         st = r.w.state
         assert (st.time, st.dt, st.it) == (sr.time, sr.dt, sr.it)
+
+
+def test_hilbert_order_walks_face_neighbours():
+    """The Hilbert keys of a uniform 2^k cube are a permutation of 0..n^3-1
+    and consecutive blocks along the curve share a face (the locality the
+    reference's Hilbert load balance relies on); on an AMR mesh the keys of
+    the leaves are distinct."""
+    from walicxe3d_b200 import problems
+    from walicxe3d_b200.mesh import BlockTree
+    for n in (2, 4, 8):
+        t = BlockTree((n, n, n), 1).roots()
+        assert sorted(t.hilbert_key(b) for b in t.leaves) == list(range(n ** 3))
+        order = t.hilbert_order()
+        for a, b in zip(order, order[1:]):
+            xa, xb = t.coords(a)[1], t.coords(b)[1]
+            assert sum(abs(i - j) for i, j in zip(xa, xb)) == 1
+    prob = problems.blast_amr(nroot=4, maxlev=3)
+    prob.tree.leaves = {int(b) for b in prob.local_blocks}
+    keys = [prob.tree.hilbert_key(int(b)) for b in prob.local_blocks]
+    assert len(set(keys)) == len(keys)

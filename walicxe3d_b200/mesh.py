@@ -132,6 +132,50 @@ class BlockTree:
         hi = np.array([(x[d] + 1) / n[d] for d in range(3)])
         return lo, hi
 
+    def hilbert_key(self, bid: int) -> int:
+        """Position along a 3-D Hilbert curve of the block's low corner at the
+        finest level, on the smallest power-of-two cube that holds the finest
+        grid (the curve of getHilbertKey, amr.f90:2031-2061).  Computed with
+        Skilling's transpose method (J. Skilling, "Programming the Hilbert
+        curve", AIP Conf. Proc. 707, 381 (2004)): undo the excess work of the
+        Gray-code walk axis by axis, Gray-encode, then interleave the bits."""
+        lev, x = self.coords(bid)
+        s = self.maxlev - lev
+        X = [v << s for v in x]
+        nmax = max(self.nb[self.maxlev])
+        bits = max(1, (nmax - 1).bit_length())
+        q = 1 << (bits - 1)
+        while q > 1:
+            p = q - 1
+            for i in range(3):
+                if X[i] & q:
+                    X[0] ^= p
+                else:
+                    t = (X[0] ^ X[i]) & p
+                    X[0] ^= t
+                    X[i] ^= t
+            q >>= 1
+        for i in range(1, 3):
+            X[i] ^= X[i - 1]
+        t = 0
+        q = 1 << (bits - 1)
+        while q > 1:
+            if X[2] & q:
+                t ^= q - 1
+            q >>= 1
+        for i in range(3):
+            X[i] ^= t
+        h = 0
+        for b in range(bits - 1, -1, -1):
+            for i in range(3):
+                h = (h << 1) | ((X[i] >> b) & 1)
+        return h
+
+    def hilbert_order(self) -> list:
+        """Leaves sorted along the Hilbert curve (the order in which the
+        reference deals blocks out to processes, HilbertOrder amr.f90:1930)."""
+        return sorted(self.leaves, key=self.hilbert_key)
+
     def morton_order(self) -> list:
         """Leaves sorted along a Morton curve of their low corner at the
         finest level."""

@@ -5,8 +5,8 @@ curve (source/amr.f90:1730-2061), exchanges the blocks that border another
 rank before each ghost fill (boundary.f90:174-291, :357-555) and reduces
 the time step with MPI_ALLREDUCE(min) (hydro_solver.f90:198).  Here:
 
-* ``make_plan`` cuts the Morton-ordered block list into contiguous,
-  equal-count shares; each rank's context holds its own blocks plus halo
+* ``make_plan`` cuts the block list, ordered along a Hilbert curve (or a
+  Morton curve), into contiguous, equal-count shares; each rank's context holds its own blocks plus halo
   copies of every face neighbour another rank owns
   (``wx3d_set_mesh_halo``).
 * ``Rank.step`` runs a main-loop iteration in parts (``wx3d_step_part``):
@@ -74,12 +74,20 @@ class Plan:
         self._slots = {b: s for s, b in enumerate(self.owned + self.halo)}
 
 
-def make_plan(local_blocks, nbroot, maxlev: int, nranks: int) -> list:
-    """Equal-count contiguous shares of the block list (Morton order), the
-    halo of each share and the send/receive lists between ranks."""
-    blocks = [int(b) for b in local_blocks if b != -1]
+def make_plan(local_blocks, nbroot, maxlev: int, nranks: int, order: str = "hilbert") -> list:
+    """Equal-count contiguous shares of the block list along a space-filling
+    curve ("hilbert", as the reference's doBalance, amr.f90:1730-1922; or
+    "morton"), the halo of each share and the send/receive lists between
+    ranks."""
     tree = BlockTree(tuple(nbroot), maxlev)
-    leaves = set(blocks)
+    leaves = {int(b) for b in local_blocks if b != -1}
+    tree.leaves = leaves
+    if order == "hilbert":
+        blocks = tree.hilbert_order()
+    elif order == "morton":
+        blocks = tree.morton_order()
+    else:
+        raise ValueError(f"unknown block order {order!r}")
     owner = {}
     bounds = np.linspace(0, len(blocks), nranks + 1).round().astype(int)
     shares = [blocks[bounds[r]:bounds[r + 1]] for r in range(nranks)]
