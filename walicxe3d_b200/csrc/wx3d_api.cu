@@ -152,7 +152,8 @@ class SlotMap {
     key_.assign(mask_ + 1, -1);
     val_.assign(mask_ + 1, -1);
   }
-  int find(long long k) const {
+  int find(long long k) const {  // -1 if absent; keys are bIDs >= 1
+    if (k < 0) return -1;
     for (size_t i = home(k);; i = (i + 1) & mask_) {
       if (key_[i] == k) return val_[i];
       if (key_[i] == -1) return -1;
@@ -185,6 +186,7 @@ class SlotMap {
       }
     }
     key_[i] = -1;
+    val_[i] = -1;
     --n_;
   }
   size_t size() const { return n_; }
