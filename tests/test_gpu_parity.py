@@ -587,3 +587,28 @@ def test_admesh_refuses_when_slots_run_out():
     with pytest.raises(WxError) as e:
         g.admesh()
     assert e.value.code == 106
+
+
+def test_admesh_with_sources_matches_oracle(ncpu):
+    """Live mesh with hydrogen ionisation and cooling_h: marking after the
+    source step (the reference marks on primitives computed before it), then
+    ten more steps with sources on the adapted mesh."""
+    prob = problems.cooling_pulse(width_pc=2.5)
+    extra = 4 * prob.nblocks
+    o = oracle.from_problem(prob, threads=ncpu, extra_slots=extra)
+    g = from_problem(prob, extra_slots=extra)
+    o.set_state(0.0, 0.0, 10, 1, 0)
+    g.set_state(time=0.0, dt=0.0, it=10, nextout=1)
+    total = np.zeros(2, int)
+    for _ in range(10):
+        o.step()
+        g.step()
+        no, ng = o.admesh(), g.admesh()
+        assert no == ng
+        assert np.array_equal(o.blocks, g.local_blocks)
+        total += ng
+    assert total[0] >= 1 and total[1] >= 1
+    occ = g.local_blocks != -1
+    Ug, Uo = g.download(g.max_blocks)[occ], o.U[occ]
+    err = rel_l1(Ug, Uo)
+    assert err.max() <= TOL, f"rel L1 per eq {err}"

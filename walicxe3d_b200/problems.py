@@ -190,6 +190,38 @@ def amr_pulse(nroot: int = 2, maxlev: int = 3, centre=(0.15, 0.15, 0.15), width:
     return _finish("amr-pulse", cfg, tree, prim_fn, steps)
 
 
+def cooling_pulse(nroot: int = 2, maxlev: int = 3, width_pc: float = 1.5, amplitude: float = 30.0,
+                  steps: int = 20) -> Problem:
+    """Live-mesh test with source terms: the ISM of snr_h (n = 1 cm^-3,
+    T = 1e4 K, neutral fraction 0.99; EOS_H_RATE + COOL_H, HLLC + minmod,
+    box 50 pc) with a Gaussian overpressure (peak amplitude x the ISM
+    pressure, half-width width_pc) in one corner, on nroot^3 root blocks all
+    refined once.  The first admesh coarsens the quiet families and refines
+    around the pulse; hydrogen ionisation and cooling act on the hot gas."""
+    mu0 = 1.3
+    cfg = Config(npassive=1, solver_type=C.SOLVER_HLLC, limiter_type=C.LIMITER_MINMOD,
+                 eos_type=C.EOS_H_RATE, cooling_type=C.COOL_H, nbroot=(nroot,) * 3, maxlev=maxlev,
+                 gamma=5.0 / 3.0, cfl=0.4, visc_eta=5.0e-3, l_sc=C.PC, d_sc=mu0 * C.AMU, v_sc=1.0e5,
+                 box=(50.0 * C.PC,) * 3, tfin=5.0e4 * C.YR, dtout=1.0e4 * C.YR)
+    tree = BlockTree(cfg.nbroot, maxlev).roots()
+    for b in sorted(tree.leaves):
+        tree.refine(b)
+    centre = np.array([7.5, 7.5, 7.5])  # pc, code units
+
+    def prim_fn(xyz):
+        dens_ism = 1.0 * C.AMU * mu0
+        pres_ism = dens_ism / (mu0 * C.AMU) * C.KB * 1.0e4
+        r2 = ((xyz - centre[None, :, None, None, None]) ** 2).sum(axis=1)
+        g = amplitude * np.exp(-r2 / width_pc ** 2)
+        prim = np.zeros((xyz.shape[0], cfg.neqtot) + xyz.shape[2:])
+        prim[:, 0] = mu0 * dens_ism / cfg.d_sc
+        prim[:, 4] = pres_ism * (1.0 + g) / cfg.p_sc
+        prim[:, 5] = 0.99 * dens_ism / cfg.d_sc
+        return prim
+
+    return _finish("cooling-pulse", cfg, tree, prim_fn, steps)
+
+
 def smooth_pulse(nroot: int = 2, amplitude: float = 0.2, width: float = 0.15, solver=C.SOLVER_HLLC,
                  limiter=C.LIMITER_MINMOD) -> Problem:
     """Smooth Gaussian density/pressure pulse at rest in a uniform medium
