@@ -311,7 +311,8 @@ def main():
     ap.add_argument("--partition", action="store_true",
                     help="strong scaling: the ranks share one mesh (halo exchange over NCCL) instead of replicas")
     ap.add_argument("--surrogate", action="store_true",
-                    help="attach the trained hrate + cooling_h surrogate (EOS_H_RATE + COOL_H workloads)")
+                    help="attach the trained surrogate (EOS_H_RATE workloads: with COOL_H both outputs, "
+                         "with table cooling its ionisation output)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

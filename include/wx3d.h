@@ -397,11 +397,15 @@ int wx3d_mlp_train(wx_mlp* mlp, int64_t n, const float* d_in, const float* d_tar
                    float lr, float* loss_per_epoch);
 
 /* Attaches (enable = 1) the surrogate to a context whose config is
- * EOS_H_RATE + COOL_H: the source step of wx3d_step / wx3d_run then uses the
- * MLP for the cells in the trust box whose bin of `trust` is non-zero, and
- * the plain integrator elsewhere.  trust[48][48][8] (nbytes = 18432) bins
- * log10(n_H dt/yr) in [-5,7) by 0.25, log10 T in [2,8) by 0.125 and x_HII
- * in eighths.  enable = 0 detaches it. */
+ * EOS_H_RATE (hydro, 1-2 passive scalars): the source step of wx3d_step /
+ * wx3d_run then uses the MLP for the cells in the trust box whose bin of
+ * `trust` is non-zero, and the plain integrator elsewhere.  With COOL_H
+ * both outputs are used (x_HII and the cooling factor; cooling_limit must
+ * be 0.5, as in training); with the table coolings (COOL_TABLE,
+ * COOL_TABLE_METAL, COOL_SCHURE) only the x_HII output replaces the hrate
+ * update and the plain table cooling follows.  trust[48][48][8]
+ * (nbytes = 18432) bins log10(n_H dt/yr) in [-5,7) by 0.25, log10 T in
+ * [2,8) by 0.125 and x_HII in eighths.  enable = 0 detaches it. */
 int wx3d_set_surrogate(wx_ctx* ctx, wx_mlp* mlp, const uint8_t* trust, int32_t nbytes, int32_t enable);
 
 /* Self-check of the Newton-refined reciprocal and square root that the flux

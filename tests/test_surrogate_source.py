@@ -14,9 +14,9 @@ MU0 = 1.3
 TRUST_SHAPE = (48, 48, 8)
 
 
-def _cfg(nblocks):
+def _cfg(nblocks, cooling=C.COOL_H):
     return C.Config(npassive=1, solver_type=C.SOLVER_HLLC, limiter_type=C.LIMITER_MINMOD,
-                    eos_type=C.EOS_H_RATE, cooling_type=C.COOL_H, nbroot=(nblocks, 1, 1), maxlev=1,
+                    eos_type=C.EOS_H_RATE, cooling_type=cooling, nbroot=(nblocks, 1, 1), maxlev=1,
                     l_sc=C.PC, d_sc=MU0 * C.AMU, v_sc=1.0e5, box=(float(nblocks) * C.PC, C.PC, C.PC))
 
 
@@ -31,9 +31,12 @@ def _cells(nblocks, seed, lo=(-3.0, 2.0), hi=(4.0, 8.0)):
 
 
 def _context(cfg, nblocks, n, T, x, dt_yr):
+    from walicxe3d_b200 import problems
     from walicxe3d_b200.solver import Walicxe3D
     w = Walicxe3D(cfg, nblocks)
     w.set_mesh(np.arange(1, nblocks + 1))
+    if cfg.cooling_type == C.COOL_TABLE:
+        w.set_cooltable(*problems.cooling_table_synthetic())
     y = 1.0 - x
     U = np.zeros((nblocks, 6) + (16, 16, 16))
     sh = (nblocks, 16, 16, 16)
@@ -194,3 +197,64 @@ def test_surrogate_ablation_speed():
     xs, Ts = _x_T(sur.download(), cfg)
     assert np.abs(xs - xp).max() <= 1.0e-3
     assert np.abs(Ts / Tp - 1.0).max() <= 1.0e-2
+
+
+def test_ionisation_surrogate_all_fallback_is_the_plain_step():
+    """EOS_H_RATE with table cooling (the colliding-winds physics): with an
+    all-zero trust table the fused kernel runs the plain hrate update and
+    the plain table cooling for every cell, bit for bit as the plain source
+    step."""
+    from walicxe3d_b200.surrogate import NPARAM
+    cfg = _cfg(2, cooling=C.COOL_TABLE)
+    n, T, x = _cells(2, seed=5)
+    a = _context(cfg, 2, n, T, x, 10.0)
+    b = _context(cfg, 2, n, T, x, 10.0)
+    b.attach_surrogate(np.zeros(NPARAM, np.float32), np.zeros(TRUST_SHAPE, np.uint8))
+    assert a.sources() == b.sources()
+    assert np.array_equal(a.download(), b.download())
+    st = b.status()
+    assert st.surrogate_cells == 0 and st.fallback_cells == 2 * C.BLOCK_CELLS
+
+
+@pytest.mark.parametrize("dt_yr", [0.3, 30.0])
+def test_ionisation_surrogate_within_tolerance(dt_yr):
+    """The trained network's x_HII output in place of the hrate update,
+    followed by the plain table cooling: gated cells within |dx_HII| <= 1e-3
+    and |dT/T| <= 1 % of the plain step, the others bit-identical."""
+    params, trust = _trained()
+    nb = 4
+    cfg = _cfg(nb, cooling=C.COOL_TABLE)
+    n, T, x = _cells(nb, seed=int(dt_yr * 100) + 3)
+    plain = _context(cfg, nb, n, T, x, dt_yr)
+    sur = _context(cfg, nb, n, T, x, dt_yr)
+    sur.attach_surrogate(params, trust)
+    plain.sources()
+    sur.sources()
+    Up, Us = plain.download(), sur.download()
+    xp, Tp = _x_T(Up, cfg)
+    xs, Ts = _x_T(Us, cfg)
+    same = (Up == Us).all(axis=1).ravel()
+    st = sur.status()
+    assert st.surrogate_cells > 0
+    assert st.fallback_cells <= int(same.sum())
+    assert np.abs(xs - xp).max() <= 1.0e-3
+    assert np.abs(Ts / Tp - 1.0).max() <= 1.0e-2
+    assert np.array_equal(Up[:, :4], Us[:, :4])
+
+
+@pytest.mark.parametrize("cooling", [C.COOL_H, C.COOL_TABLE])
+def test_dt_outside_the_training_box_is_the_plain_step(cooling):
+    """A time step below the training box (1e-3 yr, as in the reference's
+    dt ramp of a fast-wind run): the trained network is attached but no cell
+    is gated in; the kernel integrates every cell directly, bit for bit as
+    the plain source step."""
+    params, trust = _trained()
+    cfg = _cfg(2, cooling=cooling)
+    n, T, x = _cells(2, seed=8)
+    a = _context(cfg, 2, n, T, x, 1.0e-3)
+    b = _context(cfg, 2, n, T, x, 1.0e-3)
+    b.attach_surrogate(params, trust)
+    assert a.sources() == b.sources()
+    assert np.array_equal(a.download(), b.download())
+    st = b.status()
+    assert st.surrogate_cells == 0 and st.fallback_cells == 2 * C.BLOCK_CELLS

@@ -563,7 +563,8 @@ int enqueue_sources(wx_ctx* c, int mode) {
 int enqueue_surrogate(wx_ctx* c) {
   ctl_reset_dtmin_kernel<<<1, 1, 0, c->stream>>>(c->dCtl);
   WX_LAUNCHED();
-  SurrLaunch L{c->neq, c->dU, c->dBlocks, c->dWork, c->nwork, c->dCtl, c->ph, c->mlp, c->dTrust, 1, c->nsm};
+  SurrLaunch L{c->neq, c->dU, c->dBlocks, c->dWork, c->nwork, c->dCtl, c->ph, c->mlp, c->dTrust, 1, c->nsm,
+               c->dCool, c->dCool ? c->dCool + c->ncool : nullptr, c->ncool, c->nZ};
   tick(c, 3, true);
   const cudaError_t e = launch_surrogate_source(L, c->stream);
   if (e != cudaSuccess) return fail(c, WX_ERR_CUDA, "surrogate launch: %s", cudaGetErrorString(e));
@@ -1910,10 +1911,10 @@ int wx3d_set_surrogate(wx_ctx* c, wx_mlp* mlp, const uint8_t* trust, int32_t nby
   }
   if (!mlp || !trust || nbytes != TRUST_BYTES) return fail(c, WX_ERR_INVALID_ARG, "surrogate needs a %d-byte trust table", TRUST_BYTES);
   const wx_config& f = c->cfg;
-  if (f.eos_type != WX_EOS_H_RATE || f.cooling_type != WX_COOL_H || f.bfield || f.npassive < 1 || f.neqtot > 7)
-    return fail(c, WX_ERR_UNSUPPORTED, "the surrogate replaces EOS_H_RATE + COOL_H in hydro runs with 1-2 passives");
-  if (f.cooling_limit != 0.5)
-    return fail(c, WX_ERR_UNSUPPORTED, "the surrogate was trained with cooling_limit = 0.5");
+  if (f.eos_type != WX_EOS_H_RATE || f.bfield || f.npassive < 1 || f.neqtot > 7)
+    return fail(c, WX_ERR_UNSUPPORTED, "the surrogate replaces the EOS_H_RATE update in hydro runs with 1-2 passives");
+  if (f.cooling_type == WX_COOL_H && f.cooling_limit != 0.5)
+    return fail(c, WX_ERR_UNSUPPORTED, "the surrogate's cooling_h output was trained with cooling_limit = 0.5");
   if (!c->dTrust) WX_CUDA(cudaMalloc(&c->dTrust, TRUST_BYTES));
   WX_CUDA(cudaMemcpy(c->dTrust, trust, TRUST_BYTES, cudaMemcpyHostToDevice));
   c->mlp = mlp;

@@ -28,9 +28,16 @@ struct SurrLaunch {
   const uint8_t* trust;   // device [TRUST_ND][TRUST_T][TRUST_X], 1 = surrogate may be used
   int do_dt;
   int nsm;
+  // table cooling that follows the hydrogen update when the cooling type is
+  // not COOL_H (the layout of the plain source step's table)
+  const double* cool_lt;
+  const double* cool_lc;
+  int ncool;
+  int nZ;
 };
 
-// Fused updatePrims + surrogate (or plain) hrate/cooling_h + CFL minimum.
+// Fused updatePrims + surrogate (or plain) hrate, then cooling_h from the
+// network (or plain) or table cooling (plain), + CFL minimum.
 cudaError_t launch_surrogate_source(const SurrLaunch& L, cudaStream_t s);
 
 }  // namespace wx

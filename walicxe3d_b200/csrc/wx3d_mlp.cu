@@ -747,19 +747,36 @@ struct SurrParams {
   const uint8_t* __restrict__ trust;
   int do_dt;
   int* err;
+  const double* __restrict__ cool_lt;
+  const double* __restrict__ cool_lc;
+  int ncool;
+  int nZ;
 };
 
-// Plain FP64 hrate + cooling_h step of one cell (the fallback), with its
-// store and its CFL contribution.
+// Plain FP64 step of one cell (the fallback), with its store and its CFL
+// contribution: hrate + cooling_h, or hrate then table cooling, as the plain
+// source step does them (hrate.f90:101-140, then cooling_h.f90:175-246 or
+// cooling.f90:303-369 / cooling_schure.f90:134-228).
 template <int NEQ>
 __device__ __forceinline__ void fallback_cell(const SurrParams& P, int id, double dts, double& dtl, double& mloss) {
   const int slot = id >> 12, c = id & (BCELLS - 1);
   const size_t o = ((size_t)slot * NEQ) * BCELLS + c;
+  const PhysParams& ph = P.ph;
   double u[NEQ], p[NEQ];
 #pragma unroll
   for (int e = 0; e < NEQ; ++e) u[e] = P.u[o + (size_t)e * BCELLS];
-  flow2prim<NEQ, false>(u, p, P.ph.cv);
-  h_cool_step<5>(u, p, dts, P.ph, &mloss);
+  flow2prim<NEQ, false>(u, p, ph.cv);
+  if (ph.cooling == WX_COOL_H) {
+    h_cool_step<5>(u, p, dts, ph, &mloss);
+  } else {
+    const double T = calc_temp<5>(p, ph);
+    const double dh = p[0] / ph.mu0;
+    const double y0 = p[5] / dh;
+    const double y1 = h_rate_y1(T, dh, y0, dts);
+    p[5] = p[0] * y1 / ph.mu0;
+    u[5] = p[5];
+    table_cooling<NEQ, 5>(u, p, dts, ph, P.cool_lt, P.cool_lc, P.ncool, P.nZ, mloss);
+  }
   P.u[o + 4 * (size_t)BCELLS] = u[4];
   P.u[o + 5 * (size_t)BCELLS] = u[5];
   if (P.do_dt) dtl = dmin(dtl, cell_dt<NEQ, false>(p, P.blocks[slot], P.ph.gamma));
@@ -795,6 +812,11 @@ __global__ void __launch_bounds__(TILE, 4) surrogate_source_kernel(SurrParams P)
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int slot = P.work[tile / (BCELLS / TILE)];
     const int c = (int)(tile % (BCELLS / TILE)) * TILE + t;
+    if (!dt_in) {  // dt outside the training box (the same for every thread): plain step, no queue
+      fallback_cell<NEQ>(P, (slot << 12) | c, dts, dtl, mloss);
+      ++nplain;
+      continue;
+    }
     const size_t o = ((size_t)slot * NEQ) * BCELLS + c;
     double u[NEQ], p[NEQ];
 #pragma unroll
@@ -831,12 +853,19 @@ __global__ void __launch_bounds__(TILE, 4) surrogate_source_kernel(SurrParams P)
         double y1 = 1.0 - ((double)x0 + (double)y[0] * Box::SCALE_X);
         y1 = dmin(y1, 1.0 - 1.e-4);
         y1 = dmax(y1, 0.0);
-        const double cf = (double)exp10f(y[1] * (float)Box::SCALE_C);
-        mloss = dmax(mloss, 1.0 - cf);
-        p[4] *= dmin(1.0, dmax(cf, cf_min));
-        p[5] = p[0] * y1 * inv_mu0;
-        const double EK = 0.5 * p[0] * (p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
-        P.u[o + 4 * (size_t)BCELLS] = EK + ph.cv * p[4];
+        if (ph.cooling == WX_COOL_H) {  // both outputs: x_HII and the cooling factor
+          const double cf = (double)exp10f(y[1] * (float)Box::SCALE_C);
+          mloss = dmax(mloss, 1.0 - cf);
+          p[4] *= dmin(1.0, dmax(cf, cf_min));
+          p[5] = p[0] * y1 * inv_mu0;
+          const double EK = 0.5 * p[0] * (p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
+          u[4] = EK + ph.cv * p[4];
+        } else {  // x_HII from the network (the hrate update), then the plain table cooling
+          p[5] = p[0] * y1 / ph.mu0;
+          u[5] = p[5];
+          table_cooling<NEQ, 5>(u, p, dts, ph, P.cool_lt, P.cool_lc, P.ncool, P.nZ, mloss);
+        }
+        P.u[o + 4 * (size_t)BCELLS] = u[4];
         P.u[o + 5 * (size_t)BCELLS] = p[5];
         if (P.do_dt) dtl = dmin(dtl, cell_dt<NEQ, false>(p, P.blocks[slot], ph.gamma));
         ++nsur;
@@ -905,7 +934,8 @@ struct wx_mlp {
 namespace wx {
 
 cudaError_t launch_surrogate_source(const SurrLaunch& L, cudaStream_t s) {
-  SurrParams P{L.u, L.blocks, L.work, L.nwork, L.ctl, L.ph, L.mlp->pk, L.mlp->prm, L.trust, L.do_dt, L.mlp->err};
+  SurrParams P{L.u,      L.blocks,  L.work,    L.nwork,      L.ctl,       L.ph,     L.mlp->pk, L.mlp->prm,
+               L.trust,  L.do_dt,   L.mlp->err, L.cool_lt,   L.cool_lc,   L.ncool,  L.nZ};
   const long long ntiles = (long long)L.nwork * (BCELLS / TILE);
   const int grid = (int)std::min<long long>(ntiles, 4LL * L.nsm);
   if (L.neq == 6) {

@@ -198,4 +198,57 @@ __device__ __forceinline__ void h_cool_step(double* u, double* p, double dts, co
   }
 }
 
+// Table cooling of one cell after the hydrogen update: COOL_TABLE and
+// COOL_TABLE_METAL (apply_cooling, cooling.f90:303-369) and COOL_SCHURE
+// (cooling_schure.f90:134-228); updates p[4] and u[4] and folds the largest
+// fractional loss into mloss.  No-op for other cooling types or an unloaded
+// table.
+template <int NEQ, int FP>
+__device__ __forceinline__ void table_cooling(double* u, double* p, double dts, const PhysParams& ph,
+                                              const double* __restrict__ cool_lt, const double* __restrict__ cool_lc,
+                                              int ncool, int nZ, double& mloss) {
+  if ((ph.cooling == WX_COOL_TABLE || ph.cooling == WX_COOL_TABLE_METAL) && ncool >= 2) {  // cooling.f90:303-369
+    const bool metal_tab = ph.cooling == WX_COOL_TABLE_METAL;
+    const double temp = calc_temp<FP>(p, ph);
+    const double logT = log10(temp);
+    // metalpas = neqhydro + neqmhd + min(npassive, 1) (parameters.f90:318)
+    const int mp = FP + (ph.npassive >= 1 ? 1 : 0) - 1;
+    const double Tmin = metal_tab ? cool_lt[nZ + 1] : cool_lt[0];
+    if (logT >= Tmin) {
+      const double ETH = ph.cv * p[4];
+      const double EK = 0.5 * p[0] * (p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
+      double al;
+      if (metal_tab) {
+        double metal = 0.0;
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e)
+          if (e == mp) metal = fabs(p[e] / p[0]);
+        al = find_coef_metal(cool_lt, ncool, nZ, logT, metal);
+      } else {
+        al = find_coef(cool_lt, cool_lc, ncool, logT);
+      }
+      const double nd = p[0] * ph.d_sc / (ph.mui * AMU);
+      const double ce = al * (nd * nd) / (ETH * ph.e_sc);
+      double cf = exp(-ce * dts);
+      mloss = dmax(mloss, 1.0 - cf);
+      if (cf < 1.0 - ph.cooling_limit) cf = 1.0 - ph.cooling_limit;
+      if (temp * cf < 10.0) cf = 10.0 / temp;
+      p[4] = p[4] * cf;
+      u[4] = EK + ph.cv * p[4];
+    }
+  } else if (ph.cooling == WX_COOL_SCHURE && ncool == 180) {  // cooling_schure.f90:134-228
+    const double T = calc_temp<FP>(p, ph);
+    if (T > 10.0) {
+      const double Lambda0 = get_lambda_schure(cool_lt, cool_lc, T);
+      const double dens = p[0] / ph.mu0;
+      const double emtauC = exp(-2.0 * dts * dens * Lambda0 / (3.0 * KB * T));
+      double cf = (0.0 / (dens * dens * Lambda0)) * (1.0 - emtauC) + emtauC;  // gain = 0
+      mloss = dmax(mloss, 1.0 - cf);
+      if (cf < 1.0 - ph.cooling_limit) cf = 1.0 - ph.cooling_limit;
+      p[4] = p[4] * cf;
+      u[4] = ph.cv * p[4] + 0.5 * p[0] * (p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
+    }
+  }
+}
+
 }  // namespace wx
