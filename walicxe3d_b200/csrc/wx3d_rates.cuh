@@ -34,7 +34,7 @@ __device__ __forceinline__ double calc_temp(const double* p, const PhysParams& p
 __device__ __forceinline__ double h_rate_y1(double T, double dh, double y0, double dts) {
   const double xi = 1.e-4;
   const double col = 5.83e-11 * sqrt(T) * exp(-157828. / T);   // colf, hrate.f90:73
-  const double rec = 2.55e-13 * pow(1.e4 / T, 0.79);          // alpha, hrate.f90:58
+  const double rec = 2.55e-13 * exp(0.79 * log(1.e4 / T));    // alpha, hrate.f90:58: (1e4/T)^0.79
   const double a = rec + col;
   const double b = -((2.0 + xi) * rec + (1.0 + xi) * col + 0.0);
   const double c = (1.0 + xi) * rec;
@@ -50,7 +50,8 @@ __device__ __forceinline__ double h_rate_y1(double T, double dh, double y0, doub
 // betah and aloss (cooling_h.f90:42-145), Biro et al. 1999 loss rate.
 __device__ __forceinline__ double betah(double T) {
   const double a = 157890. / T;
-  return 1.133e-24 / sqrt(a) * (-0.0713 + 0.5 * log(a) + 0.640 * pow(a, -0.33333));
+  const double la = log(a);  // a^-0.33333 = exp(-0.33333 ln a)
+  return 1.133e-24 / sqrt(a) * (-0.0713 + 0.5 * la + 0.640 * exp(-0.33333 * la));
 }
 
 __device__ __forceinline__ double aloss_h(double x1, double den, double dH0, double Te0) {
@@ -81,11 +82,12 @@ __device__ __forceinline__ double aloss_h(double x1, double den, double dH0, dou
   const double erec = dmax(de * dHp * betah(Te), 0.);
   const double Tm = 1. / Te;
   const double Tm2 = Tm * Tm;
-  const double eOI = dmax(de * dOI * pow(10., 1381465 * Tm2 - 12328.69 * Tm - 19.82621), 0.);
-  const double eOII = dmax(de * dOII * pow(10., -2061075. * Tm2 - 14596.24 * Tm - 19.01402), 0.);
-  const double betaf = 1.3 * 1.42E-27 * pow(Te, 0.5);
+  const double eOI = dmax(de * dOI * exp10(1381465 * Tm2 - 12328.69 * Tm - 19.82621), 0.);
+  const double eOII = dmax(de * dOII * exp10(-2061075. * Tm2 - 14596.24 * Tm - 19.01402), 0.);
+  const double betaf = 1.3 * 1.42E-27 * sTe;  // Te^0.5
   const double HIIcool = de * dHp * betaf;
-  const double equil = (1.0455E-18 / pow(Te, 0.63)) * (1. - exp(-pow(Te * 1.E-5, 1.63))) * de * den + HIIcool;
+  // Te^0.63 and (Te 1e-5)^1.63 as exp(a ln x)
+  const double equil = (1.0455E-18 / exp(0.63 * log(Te))) * (1. - exp(-exp(1.63 * log(Te * 1.E-5)))) * de * den + HIIcool;
   double fr;
   if (Te <= 44770.) fr = 0.;
   else if (Te >= 54770.) fr = 1.;
@@ -102,14 +104,14 @@ __device__ __forceinline__ double aloss_h(double x1, double den, double dH0, dou
 __device__ __forceinline__ double find_coef(const double* __restrict__ lt, const double* __restrict__ lc, int n,
                                             double logT) {
   if (logT < lt[0]) return 0.0;
-  if (logT >= lt[n - 1]) return pow(10., lc[n - 1] + 0.5 * (logT - lt[n - 1]));
+  if (logT >= lt[n - 1]) return exp10(lc[n - 1] + 0.5 * (logT - lt[n - 1]));
   int lo = 0, hi = n - 1;  // lt[lo] <= logT < lt[hi]
   while (hi - lo > 1) {
     const int mid = (lo + hi) >> 1;
     if (lt[mid] > logT) hi = mid; else lo = mid;
   }
   const double T0 = lt[hi - 1], C0 = lc[hi - 1], T1 = lt[hi], C1 = lc[hi];
-  return pow(10., (C1 - C0) / (T1 - T0) * (logT - T0) + C0);
+  return exp10((C1 - C0) / (T1 - T0) * (logT - T0) + C0);
 }
 
 // find_coef_metal (cooling.f90:435-519) on cooltable(nT+1, nZ+1) stored row
@@ -146,13 +148,13 @@ __device__ __forceinline__ double find_coef_metal(const double* __restrict__ tab
   if (logT >= Tmax) {
     const double C0 = ct(nT, Zlo) + 0.5 * (logT - Tmax);
     const double C1 = ct(nT, Zhi) + 0.5 * (logT - Tmax);
-    return pow(10., (C1 - C0) / (Z1 - Z0) * (Z - Z0) + C0);
+    return exp10((C1 - C0) / (Z1 - Z0) * (Z - Z0) + C0);
   }
   const double TC = (logT - T0) / (T1 - T0);
   const double ZC = (Z - Z0) / (Z1 - Z0);
   const double coef = (1.0 - TC) * (1.0 - ZC) * ct(Tlo, Zlo) + (1.0 - TC) * ZC * ct(Tlo, Zhi) +
                       TC * (1.0 - ZC) * ct(Thi, Zlo) + TC * ZC * ct(Thi, Zhi);
-  return pow(10., coef);
+  return exp10(coef);
 }
 
 // get_lambda (cooling_schure.f90:102-128): 180 rows of linear T and Lambda,
