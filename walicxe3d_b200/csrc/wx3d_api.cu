@@ -229,7 +229,8 @@ struct wx_ctx {
   Tree tree;
   std::vector<int32_t> local;     // localBlocks
   std::vector<int32_t> work;      // occupied slots
-  std::vector<DevBlock> hblocks;
+  DevBlock* hblocks = nullptr;       // host copy of the device neighbour table (pinned)
+  DevBlock* hblocks_next = nullptr;  // pinned buffer the next table is built in, then swapped in
   std::vector<double> hwind;      // wind sources, 12 doubles each (wx_wind)
   double* dWind = nullptr;
   int nwork = 0;
@@ -340,7 +341,7 @@ void fill_phys(wx_ctx* c) {
 // with a coarser or finer neighbour: those ghosts would need the wind at
 // their own positions (or their sources the values before it), which only
 // a same-level neighbour provides.
-bool flag_wind_blocks(const wx_ctx* c, std::vector<DevBlock>& hb, int* bad) {
+bool flag_wind_blocks(const wx_ctx* c, DevBlock* hb, size_t n, int* bad) {
   const size_t nw = c->hwind.size() / 12;
   const double l_sc = c->cfg.l_sc;
   auto reach = [&](const double* W, const double* lo, const double* hi) {
@@ -351,7 +352,7 @@ bool flag_wind_blocks(const wx_ctx* c, std::vector<DevBlock>& hb, int* bad) {
     }
     return std::sqrt(s) <= W[6] * (1.0 + 1e-12);
   };
-  for (size_t s = 0; s < hb.size(); ++s) {
+  for (size_t s = 0; s < n; ++s) {
     DevBlock& b = hb[s];
     b.wind = 0;
     if (b.level < 1 || nw == 0) continue;
@@ -735,7 +736,10 @@ int wx3d_init(const wx_config* cfg, int32_t max_blocks, wx_ctx** out) {
   }
   if (cudaMemcpy(c->dCtl, c->hCtl, sizeof(DevCtl), cudaMemcpyHostToDevice)) return cleanup(WX_ERR_CUDA);
   c->local.assign(max_blocks, -1);
-  c->hblocks.assign(max_blocks, DevBlock{});
+  if (cudaMallocHost(&c->hblocks, sizeof(DevBlock) * (size_t)max_blocks) ||
+      cudaMallocHost(&c->hblocks_next, sizeof(DevBlock) * (size_t)max_blocks))
+    return cleanup(WX_ERR_CUDA);
+  std::memset(c->hblocks, 0, sizeof(DevBlock) * (size_t)max_blocks);
   *out = c;
   return WX_OK;
 }
@@ -750,6 +754,8 @@ int wx3d_finalize(wx_ctx* c) {
   cudaFree(c->dWind);
   cudaFree(c->dOps);
   if (c->hCtl) cudaFreeHost(c->hCtl);
+  if (c->hblocks) cudaFreeHost(c->hblocks);
+  if (c->hblocks_next) cudaFreeHost(c->hblocks_next);
   for (int i = 0; i < 64; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->own) cudaStreamDestroy(c->own);
@@ -791,7 +797,8 @@ int wx3d_set_mesh_halo(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nha
   // the table entry of every slot, independent per slot (over the host
   // cores); a face without a valid neighbour is reported as 1 + 2*face +
   // (0: no active neighbour at the finest level, 1: not one level apart)
-  std::vector<DevBlock> hb(c->max_blocks);
+  DevBlock* hb = c->hblocks_next;
+  for (int s = nslots; s < c->max_blocks; ++s) hb[s] = DevBlock{};
   std::vector<int> face_err(nslots, 0);
   auto entry = [&](int s) -> int {
     DevBlock b{};
@@ -868,13 +875,13 @@ int wx3d_set_mesh_halo(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nha
   std::copy(lb, lb + nslots, c->local.begin());
   c->nhalo = nhalo;
   int bad = -1;
-  if (!flag_wind_blocks(c, hb, &bad))
+  if (!flag_wind_blocks(c, hb, c->max_blocks, &bad))
     return fail(c, WX_ERR_UNSUPPORTED, "slot %d: a wind sphere reaches the ghost layer of a coarse/fine face; "
                 "refine the zone around the source (refineZone) further", bad);
-  c->hblocks = std::move(hb);
+  std::swap(c->hblocks, c->hblocks_next);
   c->work = std::move(work);
   c->nwork = (int)c->work.size();
-  WX_CUDA(cudaMemcpyAsync(c->dBlocks, c->hblocks.data(), sizeof(DevBlock) * c->max_blocks, cudaMemcpyHostToDevice, c->stream));
+  WX_CUDA(cudaMemcpyAsync(c->dBlocks, c->hblocks, sizeof(DevBlock) * c->max_blocks, cudaMemcpyHostToDevice, c->stream));
   if (!c->work.empty())
     WX_CUDA(cudaMemcpyAsync(c->dWork, c->work.data(), 4 * c->work.size(), cudaMemcpyHostToDevice, c->stream));
   WX_CUDA(cudaStreamSynchronize(c->stream));
@@ -916,8 +923,9 @@ int wx3d_set_winds(wx_ctx* c, int32_t nwind, const wx_wind* winds) {
   std::vector<double> prev = c->hwind;
   c->hwind = h;
   int bad = -1;
-  std::vector<DevBlock> hb = c->hblocks;
-  if (!flag_wind_blocks(c, hb, &bad)) {
+  DevBlock* hb = c->hblocks_next;
+  std::memcpy(hb, c->hblocks, sizeof(DevBlock) * (size_t)c->max_blocks);
+  if (!flag_wind_blocks(c, hb, c->max_blocks, &bad)) {
     c->hwind = prev;
     return fail(c, WX_ERR_UNSUPPORTED, "slot %d: a wind sphere reaches the ghost layer of a coarse/fine face; "
                 "refine the zone around the source (refineZone) further", bad);
@@ -929,9 +937,9 @@ int wx3d_set_winds(wx_ctx* c, int32_t nwind, const wx_wind* winds) {
     WX_CUDA(cudaMalloc(&c->dWind, sizeof(double) * h.size()));
     WX_CUDA(cudaMemcpy(c->dWind, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
   }
-  c->hblocks = hb;
+  std::swap(c->hblocks, c->hblocks_next);
   fill_phys(c);
-  WX_CUDA(cudaMemcpyAsync(c->dBlocks, c->hblocks.data(), sizeof(DevBlock) * c->max_blocks, cudaMemcpyHostToDevice,
+  WX_CUDA(cudaMemcpyAsync(c->dBlocks, c->hblocks, sizeof(DevBlock) * c->max_blocks, cudaMemcpyHostToDevice,
                           c->stream));
   WX_CUDA(cudaStreamSynchronize(c->stream));
   invalidate_graph(c);
