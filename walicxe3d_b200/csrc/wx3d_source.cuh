@@ -121,7 +121,7 @@ struct MarkParams {
 };
 
 template <int NEQ, bool MHD>
-__global__ void __launch_bounds__(256) mark_kernel(MarkParams P) {
+__global__ void __launch_bounds__(256, 4) mark_kernel(MarkParams P) {
   __shared__ double pp[3][18 * 18], pr[3][18 * 18];  // pressure and density, planes k-1..k+1
   __shared__ int first_refine;                        // first cell (loop order) reaching refineThres
   __shared__ double bmax;
