@@ -612,3 +612,43 @@ def test_admesh_with_sources_matches_oracle(ncpu):
     Ug, Uo = g.download(g.max_blocks)[occ], o.U[occ]
     err = rel_l1(Ug, Uo)
     assert err.max() <= TOL, f"rel L1 per eq {err}"
+
+
+def test_invalid_meshes_are_refused():
+    """wx3d_set_mesh refuses what the reference's tree queries would not
+    resolve (WX_ERR_MESH): a bID registered twice, a bID outside the tree, a
+    face with a level jump of two, a region no block covers; more slots than
+    the context holds is WX_ERR_INSUFICIENT_NBMAXPROC; stepping with no mesh
+    is WX_ERR_MESH.  A refused mesh leaves the previous one in place."""
+    from walicxe3d_b200._lib import WxError
+    cfg = C.Config(nbroot=(2, 2, 2), maxlev=3)
+    tree = BlockTree(cfg.nbroot, 3).roots()
+    roots = sorted(tree.leaves)
+    w = Walicxe3D(cfg, 64)
+    with pytest.raises(WxError) as e:
+        w.step()
+    assert e.value.code == 106
+    good = np.array(roots, np.int32)
+    w.set_mesh(good)
+    U = problems.smooth_pulse(nroot=2).U
+    w.upload(U)
+
+    def refused(lb, code):
+        with pytest.raises(WxError) as e:
+            w.set_mesh(np.asarray(lb, np.int32))
+        assert e.value.code == code
+
+    refused(list(roots[:-1]) + [roots[0]], 106)             # registered twice
+    refused(list(roots[:-1]) + [tree.maxid + 5], 106)        # outside the tree
+    refused(roots[1:], 106)                                  # a hole: root 1's region is uncovered
+    # level jump of two: root 1 refined twice in one octant, its neighbours left at level 1
+    t = BlockTree(cfg.nbroot, 3).roots()
+    t.refine(roots[0])
+    first = t.children(roots[0])[7]                          # the child touching the other roots
+    t.refine(first)
+    refused(sorted(t.leaves), 106)
+    refused(list(range(1, 66)), 7)                           # 65 slots > max_blocks 64
+    # the previous mesh is still in place: a step runs
+    w.set_state(time=0.0, dt=0.0, it=10, nextout=1)
+    w.step()
+    assert np.all(np.isfinite(w.download()))
