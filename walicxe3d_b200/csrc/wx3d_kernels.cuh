@@ -161,6 +161,27 @@ __device__ __forceinline__ void visc_store(const StageParams& P, const DevBlock&
 // Loads plane kk of the slab into its ring slot as primitives: the 16x16
 // physical cells, plus -- for the planes that get x/y fluxes -- the x/y ghost
 // frame (two deep for the second-order stage), gathered from the neighbours.
+// Converts one cell's conserved variables to primitives (plus, for the
+// first-order hydro stage, its sound speed and 1/rho) into ring plane pl,
+// counting the flow2prim floors of physical cells when `count`.
+template <int NEQ, bool MHD, int ORDER, int CH>
+__device__ __forceinline__ void store_cell(const PhysParams& ph, double* pl, int i, int j, const double* u, bool count,
+                                           unsigned& pf, unsigned& df, unsigned& zd) {
+  double p[NEQ], rinv;
+  const int st = flow2prim<NEQ, MHD>(u, p, ph.cv, &rinv);
+  if constexpr (CH > NEQ) {
+    pl[NEQ * Geo<ORDER>::PL + hidx<ORDER>(i, j)] = sqrt_nr(ph.gamma * p[4] * rinv);
+    pl[(NEQ + 1) * Geo<ORDER>::PL + hidx<ORDER>(i, j)] = rinv;
+  }
+  if (count) {
+    pf += (st == 1);
+    df += (st == 2);
+    zd += (st < 0);
+  }
+#pragma unroll
+  for (int e = 0; e < NEQ; ++e) pl[e * Geo<ORDER>::PL + hidx<ORDER>(i, j)] = p[e];
+}
+
 template <int NEQ, bool MHD, int ORDER, int CH>
 __device__ __forceinline__ void load_plane(const StageParams& P, const DevBlock& B, int slot, int kk, int z0, int z1,
                                            double* ring, unsigned& pf, unsigned& df, unsigned& zd) {
@@ -183,21 +204,10 @@ __device__ __forceinline__ void load_plane(const StageParams& P, const DevBlock&
       else if (side == 2) { i = r; j = d - 1; }
       else { i = r; j = NC + 2 - d; }
     }
-    double u[NEQ], p[NEQ], rinv;
+    double u[NEQ];
     if (inner && c < PLANE) load_cell<NEQ>(P.src, slot, i, j, kk, u);
     else gather_ghost<NEQ>(P.gsrc ? P.gsrc : P.src, B, slot, i, j, kk, u);
-    const int st = flow2prim<NEQ, MHD>(u, p, ph.cv, &rinv);
-    if constexpr (CH > NEQ) {
-      pl[NEQ * Geo<ORDER>::PL + hidx<ORDER>(i, j)] = sqrt_nr(ph.gamma * p[4] * rinv);
-      pl[(NEQ + 1) * Geo<ORDER>::PL + hidx<ORDER>(i, j)] = rinv;
-    }
-    if (c < PLANE && inner && frame) {
-      pf += (st == 1);
-      df += (st == 2);
-      zd += (st < 0);
-    }
-#pragma unroll
-    for (int e = 0; e < NEQ; ++e) pl[e * Geo<ORDER>::PL + hidx<ORDER>(i, j)] = p[e];
+    store_cell<NEQ, MHD, ORDER, CH>(ph, pl, i, j, u, c < PLANE && inner && frame, pf, df, zd);
   }
 }
 
