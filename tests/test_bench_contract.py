@@ -1,0 +1,30 @@
+"""The benchmark's JSON line: the reference arm (the C++ FP64 restatement on
+the host cores) runs without a GPU, so its line is checked here key by key;
+the device arm's line shares the same base keys."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reference_arm_prints_one_contract_line():
+    out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--workload", "sedov64", "--steps", "2",
+                          "--warmup", "3"], cwd=ROOT, capture_output=True, text=True, timeout=600, check=True)
+    lines = [ln for ln in out.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config"):
+        assert k in d, k
+    assert d["metric"] == d["unit"] == "Mcell-updates/s"
+    assert d["steps"] == 2 and d["warmup"] >= 3 and d["n_gpus"] == 1
+    assert d["higher_is_better"] is True and d["dtype"] == "f64" and d["value"] > 0
+    assert d["config"]["workload"] == "sedov64" and d["config"]["cells"] == 64 * 4096
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    e2e = d["e2e"]
+    assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
+    assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
