@@ -1694,32 +1694,6 @@ void check_proximity(const Tree& T, const SlotList& L, std::vector<int>& flags, 
     }
 }
 
-// Splits an operation list (9 slots each: father, then 8 children or
-// siblings) into runs in which no op writes a slot that an earlier op of the
-// same run reads; returns the run boundaries.
-std::vector<int> conflict_free_runs(const std::vector<int32_t>& ops, bool refine) {
-  std::vector<int> cuts{0};
-  std::unordered_map<int, int> reads;  // slot -> reading op, current run
-  const int n = (int)ops.size() / 9;
-  for (int o = 0; o < n; ++o) {
-    const int32_t* p = ops.data() + 9 * o;
-    bool clash = false;
-    if (refine) {
-      for (int c = 1; c <= 8 && !clash; ++c) clash = reads.count(p[c]) != 0;
-    } else {
-      clash = reads.count(p[0]) != 0;
-    }
-    if (clash) {
-      cuts.push_back(o);
-      reads.clear();
-    }
-    if (refine) reads[p[0]] = o;
-    else for (int c = 1; c <= 8; ++c) reads[p[c]] = o;
-  }
-  cuts.push_back(n);
-  return cuts;
-}
-
 }  // namespace
 
 int wx3d_admesh(wx_ctx* c, int32_t nbmax, int32_t* lb, int32_t* counts) {
@@ -1788,21 +1762,29 @@ int wx3d_admesh(wx_ctx* c, int32_t nbmax, int32_t* lb, int32_t* counts) {
     counts[1] = ncoarse;
   }
   if (rops.empty() && cops.empty()) return WX_OK;  // the mesh and the state stay as they are
-  // data: refinements, then coarsenings, in conflict-free runs
+  // data: refinements, then coarsenings.  Each pass first copies the blocks
+  // it reads (fathers, or siblings) from U into UP at the same slots -- UP
+  // holds nothing between steps, the next predictor overwrites it -- then
+  // reads them there, so slots freed and taken again within the pass need no
+  // ordering.
   {
     if (!c->dOps) WX_CUDA(cudaMalloc(&c->dOps, sizeof(int32_t) * 9 * (size_t)c->max_blocks));
     for (int pass = 0; pass < 2; ++pass) {
       const std::vector<int32_t>& ops = pass == 0 ? rops : cops;
       if (ops.empty()) continue;
       WX_CUDA(cudaMemcpyAsync(c->dOps, ops.data(), 4 * ops.size(), cudaMemcpyHostToDevice, c->stream));
-      const std::vector<int> cut = conflict_free_runs(ops, pass == 0);
-      for (size_t r = 0; r + 1 < cut.size(); ++r)
-        for (int o = cut[r]; o < cut[r + 1]; o += 8000) {
-          const int n = std::min(8000, cut[r + 1] - o);
-          if (pass == 0) refine_batch_kernel<<<dim3(16, 8 * n), 256, 0, c->stream>>>(c->dU, c->neq, c->dOps + 9 * o);
-          else coarsen_batch_kernel<<<dim3(4, 8 * n), 256, 0, c->stream>>>(c->dU, c->neq, c->dOps + 9 * o);
-          WX_LAUNCHED();
-        }
+      const int nops = (int)(ops.size() / 9), per = pass == 0 ? 1 : 8, off = pass == 0 ? 0 : 1;
+      for (int o = 0; o < nops; o += 8000) {
+        const int n = std::min(8000, nops - o);
+        stage_blocks_kernel<<<dim3(8, per * n), 256, 0, c->stream>>>(c->dU, c->dUP, c->neq, c->dOps + 9 * o, per, off);
+        WX_LAUNCHED();
+      }
+      for (int o = 0; o < nops; o += 8000) {
+        const int n = std::min(8000, nops - o);
+        if (pass == 0) refine_batch_kernel<<<dim3(16, 8 * n), 256, 0, c->stream>>>(c->dUP, c->dU, c->neq, c->dOps + 9 * o);
+        else coarsen_batch_kernel<<<dim3(4, 8 * n), 256, 0, c->stream>>>(c->dUP, c->dU, c->neq, c->dOps + 9 * o);
+        WX_LAUNCHED();
+      }
       WX_CUDA(cudaStreamSynchronize(c->stream));  // dOps is refilled by the next pass
     }
   }

@@ -239,10 +239,24 @@ __global__ void coarsen_kernel(double* __restrict__ u, int neq, int father, Slot
 }
 
 // Batched forms for admesh: op = [father, child0..child7] (9 slots), one
-// CTA row per (op, child) or (op, sibling).  No slot is written by one op of
-// a batch and read by another: the host cuts batches where a freed slot is
-// taken again.
-__global__ void refine_batch_kernel(double* __restrict__ u, int neq, const int32_t* __restrict__ ops) {
+// CTA row per (op, child) or (op, sibling).  A slot freed by one op may be
+// taken by a later one, so the blocks a pass reads are first copied (same
+// slots) into a scratch array by stage_blocks_kernel, and the pass reads the
+// scratch and writes the state: no op writes what another op reads.
+//
+// stage_blocks_kernel copies, for every op, the `per` slots starting at
+// entry `off` (the father: per 1, off 0; the siblings: per 8, off 1).
+__global__ void stage_blocks_kernel(const double* __restrict__ from, double* __restrict__ to, int neq,
+                                    const int32_t* __restrict__ ops, int per, int off) {
+  const int item = blockIdx.y;
+  const int slot = ops[9 * (item / per) + off + item % per];
+  const size_t base = (size_t)slot * neq * BCELLS;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < BCELLS * neq; c += gridDim.x * blockDim.x)
+    to[base + c] = from[base + c];
+}
+
+__global__ void refine_batch_kernel(const double* __restrict__ from, double* __restrict__ u, int neq,
+                                    const int32_t* __restrict__ ops) {
   const int op = blockIdx.y >> 3, cc = blockIdx.y & 7;
   const int father = ops[9 * op], child = ops[9 * op + 1 + cc];
   const int sx = cc & 1, sy = (cc >> 1) & 1, sz = (cc >> 2) & 1;
@@ -250,11 +264,12 @@ __global__ void refine_batch_kernel(double* __restrict__ u, int neq, const int32
     const int e = c / BCELLS, r = c % BCELLS;
     const int i = (r & 15) + 1, j = ((r >> 4) & 15) + 1, k = (r >> 8) + 1;
     const int ip = 8 * sx + (i + 1) / 2, jp = 8 * sy + (j + 1) / 2, kp = 8 * sz + (k + 1) / 2;
-    u[cell_off(child, neq, e, i, j, k)] = u[cell_off(father, neq, e, ip, jp, kp)];
+    u[cell_off(child, neq, e, i, j, k)] = from[cell_off(father, neq, e, ip, jp, kp)];
   }
 }
 
-__global__ void coarsen_batch_kernel(double* __restrict__ u, int neq, const int32_t* __restrict__ ops) {
+__global__ void coarsen_batch_kernel(const double* __restrict__ from, double* __restrict__ u, int neq,
+                                     const int32_t* __restrict__ ops) {
   const int op = blockIdx.y >> 3, sib = blockIdx.y & 7;
   const int father = ops[9 * op], child = ops[9 * op + 1 + sib];
   const int sx = sib & 1, sy = (sib >> 1) & 1, sz = (sib >> 2) & 1;
@@ -265,7 +280,7 @@ __global__ void coarsen_batch_kernel(double* __restrict__ u, int neq, const int3
     double s = 0.0;
     for (int kk = k1; kk <= k1 + 1; ++kk)
       for (int jj = j1; jj <= j1 + 1; ++jj)
-        for (int ii = i1; ii <= i1 + 1; ++ii) s += u[cell_off(child, neq, e, ii, jj, kk)];
+        for (int ii = i1; ii <= i1 + 1; ++ii) s += from[cell_off(child, neq, e, ii, jj, kk)];
     u[cell_off(father, neq, e, i + 8 * sx, j + 8 * sy, k + 8 * sz)] = s / 8.0;
   }
 }
