@@ -493,6 +493,23 @@ def test_cooling_variants_match_oracle(ctype, ncpu):
     assert g.download()[:, 4].sum() < (1.0 - 1e-4) * E0
 
 
+@pytest.mark.parametrize("eos", [C.EOS_ADIABATIC, C.EOS_TWOTEMP])
+def test_table_cooling_with_each_temperature_law(eos, ncpu):
+    """calcTemp's other equations of state (hydro_core.f90:231-270) feeding
+    the table cooling: ADIABATIC, and TWOTEMP, whose mean molecular weight
+    switches from mu0 to mui above ion_thres (1e4 K; the blob spans 1e4 to
+    3e7 K, so both branches are taken)."""
+    prob = problems.cooling_blob(C.COOL_TABLE, nroot=2, eos=eos)
+    o = oracle.from_problem(prob, threads=ncpu)
+    g = from_problem(prob)
+    E0 = prob.U[:, 4].sum()
+    for _ in range(12):
+        o.step()
+        g.step()
+    check(o, g, prob)
+    assert g.download()[:, 4].sum() < (1.0 - 1e-4) * E0
+
+
 @pytest.mark.parametrize("shape", ["1-fused", "1", "2", "8"])
 @pytest.mark.parametrize("solver", [C.SOLVER_HLLD, C.SOLVER_HLL1])
 def test_field_cd_matches_oracle(shape, solver, ncpu):

@@ -488,16 +488,17 @@ def schure_table_synthetic() -> np.ndarray:
     return data
 
 
-def cooling_blob(cooling_type: int, nroot: int = 4, steps: int = 10) -> Problem:
+def cooling_blob(cooling_type: int, nroot: int = 4, steps: int = 10, eos: int = C.EOS_SINGLE_SPECIE) -> Problem:
     """A hot, dense blob in a warm medium, in physical units (box 1 pc,
     l_sc = pc, d_sc = 1.3 amu, v_sc = 1 km/s): n from 10 to 1000 cm^-3 and T
     from 1e4 to 3e7 K, smooth, with a metallicity passive scalar of 0.05 to
     4 times the density (COOL_TABLE_METAL reads it), slow expansion.  For
     COOL_TABLE, COOL_TABLE_METAL and COOL_SCHURE with synthetic tables;
-    cooling removes percents of the thermal energy per step."""
+    cooling removes percents of the thermal energy per step.  `eos` selects
+    the temperature calcTemp gives the cooling (single specie by default)."""
     mu0 = 1.3
     cfg = Config(npassive=1, solver_type=C.SOLVER_HLLC, limiter_type=C.LIMITER_MINMOD,
-                 eos_type=C.EOS_SINGLE_SPECIE, cooling_type=cooling_type, nbroot=(nroot,) * 3, maxlev=1,
+                 eos_type=eos, cooling_type=cooling_type, nbroot=(nroot,) * 3, maxlev=1,
                  gamma=5.0 / 3.0, cfl=0.4, visc_eta=5.0e-3, l_sc=C.PC, d_sc=mu0 * C.AMU, v_sc=1.0e5,
                  box=(C.PC,) * 3, tfin=1.0e9 * C.YR, dtout=1.0e9 * C.YR)
     tree = BlockTree(cfg.nbroot, 1).roots()
