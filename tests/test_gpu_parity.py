@@ -527,10 +527,12 @@ def test_field_cd_matches_oracle(shape, solver, ncpu):
     check(o, g, prob)
 
 
-def test_field_cd_on_a_refined_mesh_matches_oracle(ncpu):
-    """Field-CD on a two-level mesh: the electric field of the ghost cells
-    comes through coarse/fine faces (injected or averaged primitives)."""
-    prob = problems.orszag_tang_3d(nroot=4, maxlev=2)
+@pytest.mark.parametrize("flux_cd", [True, False])
+def test_field_cd_on_a_refined_mesh_matches_oracle(flux_cd, ncpu):
+    """MHD on a two-level mesh, with field-CD or the Powell 8-wave source:
+    the electric field (or div B) of the ghost cells comes through
+    coarse/fine faces (injected or averaged primitives)."""
+    prob = problems.orszag_tang_3d(nroot=4, maxlev=2, flux_cd=flux_cd)
     assert {prob.tree.level(int(b)) for b in prob.local_blocks} == {1, 2}
     o, g = run_both(prob, 10, ncpu)
     check(o, g, prob)
