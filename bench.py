@@ -246,7 +246,8 @@ def live_mesh_leg(prob, args, stream):
 
 def run_partition(args, prob, rank, world, dist):
     """One mesh shared by the ranks (walicxe3d_b200.partition): each owns a
-    Morton share plus halo copies, exchanged over NCCL between the stages;
+    Hilbert share plus halo copies whose face slabs are exchanged over NCCL
+    between the stages;
     timed with CUDA events on the library stream, max over ranks."""
     import torch
     from walicxe3d_b200.partition import Rank, TorchDist, make_plan
@@ -289,8 +290,11 @@ def run_partition(args, prob, rank, world, dist):
                 "dtype": "f64", "data": "synthetic",
                 "config": {"workload": args.workload, "description": WORKLOADS[args.workload]["desc"],
                            "blocks": prob.nblocks, "cells": prob.cells,
-                           "parallelism": f"block partition x{world} (Morton shares, halo blocks over NCCL)",
-                           "halo_blocks": [len(p.halo) for p in plans]}}
+                           "parallelism": f"block partition x{world} (Hilbert shares, halo face slabs over NCCL)",
+                           "halo_blocks": [len(p.halo) for p in plans],
+                           "halo_face_slabs": [sum(len(v) for v in p.recv_faces.values()) for p in plans],
+                           "exchange_bytes_per_step": 2 * sum(sum(len(v) for v in p.recv_faces.values())
+                                                              for p in plans) * prob.cfg.neqtot * 1024 * 8}}
         print(json.dumps(line), flush=True)
     r.w.close()
     if dist is not None:

@@ -440,6 +440,18 @@ int wx3d_set_dtmin(wx_ctx* ctx, double dtmin);
 int wx3d_pack_blocks(wx_ctx* ctx, int32_t array, int32_t n, const int32_t* slots, double* d_buf);
 int wx3d_unpack_blocks(wx_ctx* ctx, int32_t array, int32_t n, const int32_t* slots, const double* d_buf);
 
+/* As wx3d_pack_blocks/wx3d_unpack_blocks for the four cell layers of each
+ * block next to one of its faces (faces[i]: 0..5 = left, right, front,
+ * back, bottom, top): n*neqtot*1024 doubles, item after item.  Whatever a
+ * neighbouring process reads of a halo block lies within those layers
+ * across the faces it shares with the halo block: two layers for a
+ * same-level ghost fill, one coarse layer for injection, four fine layers
+ * for the averages of a coarser block's ghosts (boundary.f90:329-540).  The
+ * same halo refresh as whole blocks, at a quarter of the bytes per face. */
+int wx3d_pack_faces(wx_ctx* ctx, int32_t array, int32_t n, const int32_t* slots, const int32_t* faces, double* d_buf);
+int wx3d_unpack_faces(wx_ctx* ctx, int32_t array, int32_t n, const int32_t* slots, const int32_t* faces,
+                      const double* d_buf);
+
 /* Human-readable text of a status code and of the context's last error. */
 const char* wx3d_error_string(int32_t code);
 int wx3d_last_error(wx_ctx* ctx, char* buf, int32_t len);

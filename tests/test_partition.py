@@ -12,7 +12,7 @@ import torch.multiprocessing as mp
 from walicxe3d_b200 import config as C
 from walicxe3d_b200 import problems
 from walicxe3d_b200.mesh import BlockTree
-from walicxe3d_b200.partition import face_neighbours, make_plan
+from walicxe3d_b200.partition import FACE_CELLS, face_neighbours, face_neighbours_by_face, make_plan
 
 
 def _amr():
@@ -35,6 +35,18 @@ def test_plan_covers_every_neighbour_and_is_symmetric():
             for q, bids in p.recv.items():
                 assert plans[q].send[p.rank] == bids
                 assert set(bids) <= set(plans[q].owned)
+            # face slabs: the same halo blocks, each face bordering this rank's blocks
+            for q, items in p.recv_faces.items():
+                assert plans[q].send_faces[p.rank] == items
+                assert {b for b, _ in items} == set(p.recv[q])
+                for b, f in items:
+                    assert face_neighbours_by_face(tree, leaves, b)[f] & set(p.owned)
+            for b in p.owned:
+                for f, across in enumerate(face_neighbours_by_face(tree, leaves, b)):
+                    for h in across & set(p.halo):
+                        # b reads h across h's opposite face: that slab is received
+                        g = f ^ 1
+                        assert (h, g) in {it for its in p.recv_faces.values() for it in its}
 
 
 def test_face_neighbours_of_a_three_level_mesh_are_levels_apart_by_one():
@@ -61,8 +73,17 @@ class _CpuRank:
         for i, b in enumerate(bids):
             self.data[b] = buf[i * self.neq * 4096:(i + 1) * self.neq * 4096].clone()
 
+    def pack_faces(self, array, items, buf):
+        n = self.neq * FACE_CELLS
+        buf.copy_(torch.cat([self.data[b][:n] for b, _ in items]))
 
-def _exchange_worker(rank, world, port, q):
+    def unpack_faces(self, array, items, buf):
+        n = self.neq * FACE_CELLS
+        for i, (b, f) in enumerate(items):
+            self.data[(b, f)] = buf[i * n:(i + 1) * n].clone()
+
+
+def _exchange_worker(rank, world, port, q, faces):
     import torch.distributed as dist
     from walicxe3d_b200.partition import TorchDist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
@@ -73,8 +94,12 @@ def _exchange_worker(rank, world, port, q):
         plans = make_plan(prob.local_blocks, prob.cfg.nbroot, prob.cfg.maxlev, world)
         values = {int(b): float(b) for b in prob.local_blocks}
         r = _CpuRank(plans[rank], 2, values)
-        TorchDist(r, device="cpu").exchange(0)
-        ok = all(bool(torch.all(r.data[b] == float(b))) for b in plans[rank].halo)
+        TorchDist(r, device="cpu", faces=faces).exchange(0)
+        if faces:
+            items = [it for its in plans[rank].recv_faces.values() for it in its]
+            ok = bool(items) and all(bool(torch.all(r.data[(b, f)] == float(b))) for b, f in items)
+        else:
+            ok = all(bool(torch.all(r.data[b] == float(b))) for b in plans[rank].halo)
         t = torch.tensor([float(rank + 1)], dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MIN)
         q.put((rank, ok, len(plans[rank].halo), float(t.item())))
@@ -82,11 +107,12 @@ def _exchange_worker(rank, world, port, q):
         dist.destroy_process_group()
 
 
-def test_halo_exchange_between_two_gloo_processes():
+@pytest.mark.parametrize("faces", [False, True])
+def test_halo_exchange_between_two_gloo_processes(faces):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    port = 29611
-    procs = [ctx.Process(target=_exchange_worker, args=(r, 2, port, q)) for r in range(2)]
+    port = 29611 + int(faces)
+    procs = [ctx.Process(target=_exchange_worker, args=(r, 2, port, q, faces)) for r in range(2)]
     for p in procs:
         p.start()
     res = [q.get(timeout=120) for _ in procs]
@@ -96,17 +122,19 @@ def test_halo_exchange_between_two_gloo_processes():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name,nranks", [("amr", 2), ("amr", 3), ("snr-h", 2), ("brio-wu", 2)])
-def test_partitioned_step_equals_single_context(name, nranks):
-    """Ranks on one device exchanging their halo blocks reproduce the
-    single-context run bit for bit: same fluxes per block, same global dt."""
+@pytest.mark.parametrize("name,nranks,faces", [("amr", 2, True), ("amr", 3, True), ("snr-h", 2, True),
+                                               ("brio-wu", 2, True), ("amr", 3, False)])
+def test_partitioned_step_equals_single_context(name, nranks, faces):
+    """Ranks on one device exchanging their halo face slabs (or whole halo
+    blocks) reproduce the single-context run bit for bit: same fluxes per
+    block, same global dt."""
     from walicxe3d_b200.partition import LocalGroup, Rank
     from walicxe3d_b200.solver import from_problem
     prob = {"amr": _amr, "snr-h": lambda: problems.snr_h(nroot=2, maxlev=2),
             "brio-wu": lambda: problems.brio_wu(4)}[name]()
     ref = from_problem(prob)
     plans = make_plan(prob.local_blocks, prob.cfg.nbroot, prob.cfg.maxlev, nranks)
-    group = LocalGroup([Rank(prob, p) for p in plans])
+    group = LocalGroup([Rank(prob, p) for p in plans], faces=faces)
     for _ in range(6):
         ref.step()
         group.step()

@@ -34,6 +34,8 @@ _SIGNATURES = {
     "wx3d_set_dtmin": (ctypes.c_int, [c_void_p, ctypes.c_double]),
     "wx3d_pack_blocks": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_void_p]),
     "wx3d_unpack_blocks": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_void_p]),
+    "wx3d_pack_faces": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p, c_void_p]),
+    "wx3d_unpack_faces": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p, c_void_p]),
     "wx3d_set_zsplit": (ctypes.c_int, [c_void_p, ctypes.c_int32]),
     "wx3d_set_fusion": (ctypes.c_int, [c_void_p, ctypes.c_int32]),
     "wx3d_set_winds": (ctypes.c_int, [c_void_p, ctypes.c_int32, c_double_p]),

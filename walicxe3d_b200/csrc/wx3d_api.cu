@@ -221,6 +221,7 @@ struct wx_ctx {
   int32_t* dWork = nullptr;
   int32_t* dFlags = nullptr;
   int32_t* dOps = nullptr;   // admesh: refine/coarsen operations, 9 slots each
+  int32_t* dItems = nullptr; // face-slab exchange: (slot, face) pairs
   DevCtl* dCtl = nullptr;
   DevCtl* hCtl = nullptr;   // pinned mirror
   double* dCool = nullptr;  // COOL_TABLE [2][ncool]; METAL [ncool+1][nZ+1]; SCHURE [2][180]
@@ -753,6 +754,7 @@ int wx3d_finalize(wx_ctx* c) {
   cudaFree(c->dTrust);
   cudaFree(c->dWind);
   cudaFree(c->dOps);
+  cudaFree(c->dItems);
   if (c->hCtl) cudaFreeHost(c->hCtl);
   if (c->hblocks) cudaFreeHost(c->hblocks);
   if (c->hblocks_next) cudaFreeHost(c->hblocks_next);
@@ -1017,6 +1019,40 @@ int wx3d_pack_blocks(wx_ctx* c, int32_t array, int32_t n, const int32_t* slots, 
 
 int wx3d_unpack_blocks(wx_ctx* c, int32_t array, int32_t n, const int32_t* slots, const double* d_buf) {
   return copy_blocks(c, array, n, slots, const_cast<double*>(d_buf), false);
+}
+
+static int copy_faces(wx_ctx* c, int32_t array, int32_t n, const int32_t* slots, const int32_t* faces, double* buf,
+                      bool pack) {
+  if (!c || n < 0 || (n > 0 && (!slots || !faces || !buf)) || (array != 0 && array != 1)) return WX_ERR_INVALID_ARG;
+  if (n == 0) return WX_OK;
+  if (n > 6 * c->max_blocks) return fail(c, WX_ERR_INVALID_ARG, "%d face slabs > 6 x max_blocks", n);
+  std::vector<int32_t> items(2 * (size_t)n);
+  for (int b = 0; b < n; ++b) {
+    if (slots[b] < 0 || slots[b] >= c->max_blocks) return fail(c, WX_ERR_INVALID_ARG, "slot %d out of range", slots[b]);
+    if (faces[b] < 0 || faces[b] > 5) return fail(c, WX_ERR_INVALID_ARG, "face %d out of 0..5", faces[b]);
+    items[2 * b] = slots[b];
+    items[2 * b + 1] = faces[b];
+  }
+  if (!c->dItems) WX_CUDA(cudaMalloc(&c->dItems, sizeof(int32_t) * 12 * (size_t)c->max_blocks));
+  WX_CUDA(cudaMemcpyAsync(c->dItems, items.data(), 4 * items.size(), cudaMemcpyHostToDevice, c->stream));
+  double* a = array == 0 ? c->dU : c->dUP;
+  for (int o = 0; o < n; o += 60000) {
+    const int m = std::min(60000, n - o);
+    face_slab_kernel<<<dim3(4, m), 256, 0, c->stream>>>(a, c->dItems + 2 * o, c->neq,
+                                                        buf + (size_t)o * c->neq * FACE_LAYERS * NC * NC, pack ? 1 : 0);
+    WX_LAUNCHED();
+  }
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  return WX_OK;
+}
+
+int wx3d_pack_faces(wx_ctx* c, int32_t array, int32_t n, const int32_t* slots, const int32_t* faces, double* d_buf) {
+  return copy_faces(c, array, n, slots, faces, d_buf, true);
+}
+
+int wx3d_unpack_faces(wx_ctx* c, int32_t array, int32_t n, const int32_t* slots, const int32_t* faces,
+                      const double* d_buf) {
+  return copy_faces(c, array, n, slots, faces, const_cast<double*>(d_buf), false);
 }
 
 int wx3d_set_fusion(wx_ctx* c, int32_t on) {

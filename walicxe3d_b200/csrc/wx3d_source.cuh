@@ -344,6 +344,30 @@ __global__ void native_to_fortran(const double* __restrict__ u, double* __restri
 // block as U(nb, :, 1:16, 1:16, 1:16): the equation index fastest, then i,
 // j, k.  pack: slots slot0.. of the native state -> nb consecutive blocks
 // of that order; unpack: the reverse.
+// The four cell layers of a block next to one of its faces (item = slot,
+// face 0..5 = left, right, front, back, bottom, top), neq x 4 x 16 x 16
+// doubles per item: per equation the layers in index order along the face
+// normal, then the two transverse indices; pack copies them from `a` to
+// `buf`, unpack back.
+constexpr int FACE_LAYERS = 4;
+__global__ void face_slab_kernel(double* __restrict__ a, const int32_t* __restrict__ items, int neq,
+                                 double* __restrict__ buf, int pack) {
+  const int item = blockIdx.y;
+  const int slot = items[2 * item], f = items[2 * item + 1];
+  const int ax = f >> 1, side = f & 1;
+  const int per = neq * FACE_LAYERS * NC * NC;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < per; c += gridDim.x * blockDim.x) {
+    const int e = c / (FACE_LAYERS * NC * NC), r = c % (FACE_LAYERS * NC * NC);
+    const int l = r / (NC * NC), t2 = (r / NC) % NC + 1, t1 = r % NC + 1;
+    const int g = side ? NC - FACE_LAYERS + 1 + l : 1 + l;
+    const int i = ax == 0 ? g : t1, j = ax == 1 ? g : (ax == 0 ? t1 : t2), k = ax == 2 ? g : t2;
+    double* cell = a + cell_off(slot, neq, e, i, j, k);
+    double* b = buf + (size_t)item * per + c;
+    if (pack) *b = *cell;
+    else *cell = *b;
+  }
+}
+
 __global__ void pack_bin_kernel(const double* __restrict__ u, const int32_t* __restrict__ slots, int nb, int neq,
                                 double* __restrict__ out) {
   const long long n = (long long)nb * BCELLS * neq;

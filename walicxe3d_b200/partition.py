@@ -11,7 +11,9 @@ the time step with MPI_ALLREDUCE(min) (hydro_solver.f90:198).  Here:
   (``wx3d_set_mesh_halo``).
 * ``Rank.step`` runs a main-loop iteration in parts (``wx3d_step_part``):
   global CFL minimum, U halo exchange, predictor, UP halo exchange,
-  corrector + viscous step, source terms.  Halo blocks travel whole.
+  corrector + viscous step, source terms.  Halo blocks travel as the four
+  cell layers next to each face that borders the receiver
+  (``wx3d_pack_faces``), or whole.
 * Transports: ``LocalGroup`` moves the blocks of several ranks that live in
   one process on one device (the test of the partitioned algorithm on a
   single GPU); ``TorchDist`` uses torch.distributed (NCCL between GPUs:
@@ -30,13 +32,14 @@ import numpy as np
 from . import _lib
 from .mesh import BlockTree
 
+FACE_CELLS = 4 * 16 * 16   # cells of one face slab (wx3d_pack_faces)
 
-def face_neighbours(tree: BlockTree, leaves: set, bid: int) -> set:
-    """Active blocks across the six faces of ``bid``: same level, the
-    coarser block covering the region, or the four finer blocks touching
-    the face (the cases of amr.f90:539-631)."""
-    out = set()
-    lev, x = tree.coords(bid)
+
+def face_neighbours_by_face(tree: BlockTree, leaves: set, bid: int) -> list:
+    """Active blocks across each of the six faces of ``bid`` (LEFT..TOP):
+    same level, the coarser block covering the region, or the four finer
+    blocks touching the face (the cases of amr.f90:539-631)."""
+    out = [set() for _ in range(6)]
     for f in range(6):
         n = tree.neighbour_region(bid, f)
         if n is None:
@@ -45,23 +48,32 @@ def face_neighbours(tree: BlockTree, leaves: set, bid: int) -> set:
         while b != -1 and b not in leaves:
             b = tree.father(b)
         if b != -1:
-            out.add(b)
+            out[f].add(b)
             continue
         ax, side = f // 2, f % 2
         for c in tree.children(n):
             _, cx = tree.coords(c)
             if (cx[ax] & 1) == (0 if side else 1):
-                out.add(c)
+                out[f].add(c)
     return out
+
+
+def face_neighbours(tree: BlockTree, leaves: set, bid: int) -> set:
+    """Active blocks across any of the six faces of ``bid``."""
+    return set().union(*face_neighbours_by_face(tree, leaves, bid))
 
 
 @dataclass
 class Plan:
     rank: int
-    owned: list                                # bIDs, in the global (Morton) order
+    owned: list                                # bIDs, in the order of the space-filling curve
     halo: list                                 # bIDs of other ranks' blocks this rank reads
     send: dict = field(default_factory=dict)   # peer -> owned bIDs the peer needs
     recv: dict = field(default_factory=dict)   # peer -> halo bIDs that peer sends
+    # the same exchange as (bID, face) slabs: the faces of each halo block
+    # that border the receiver's own blocks, in the same order on both sides
+    send_faces: dict = field(default_factory=dict)
+    recv_faces: dict = field(default_factory=dict)
 
     @property
     def local_blocks(self) -> np.ndarray:
@@ -106,6 +118,10 @@ def make_plan(local_blocks, nbroot, maxlev: int, nranks: int, order: str = "hilb
             q = owner[b]
             p.recv.setdefault(q, []).append(b)
             plans[q].send.setdefault(p.rank, []).append(b)
+            for f, across in enumerate(face_neighbours_by_face(tree, leaves, b)):
+                if any(owner[n] == p.rank for n in across):
+                    p.recv_faces.setdefault(q, []).append((b, f))
+                    plans[q].send_faces.setdefault(p.rank, []).append((b, f))
     return plans
 
 
@@ -155,6 +171,27 @@ class Rank:
                                                  s.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
                                                  ctypes.c_void_p(dbuf.data_ptr())), "wx3d_unpack_blocks", self.w.ctx)
 
+    def pack_faces(self, array: int, items, dbuf):
+        s = self._slots([b for b, _ in items])
+        f = np.asarray([f for _, f in items], dtype=np.int32)
+        _lib.check(self.w.lib.wx3d_pack_faces(self.w.ctx, array, len(s), s.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                              f.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                              ctypes.c_void_p(dbuf.data_ptr())), "wx3d_pack_faces", self.w.ctx)
+
+    def unpack_faces(self, array: int, items, dbuf):
+        s = self._slots([b for b, _ in items])
+        f = np.asarray([f for _, f in items], dtype=np.int32)
+        _lib.check(self.w.lib.wx3d_unpack_faces(self.w.ctx, array, len(s),
+                                                s.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                                f.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                                ctypes.c_void_p(dbuf.data_ptr())), "wx3d_unpack_faces", self.w.ctx)
+
+    def exchange_bytes(self, faces: bool = True) -> int:
+        """Bytes this rank sends per exchange (one array)."""
+        if faces:
+            return sum(len(v) for v in self.plan.send_faces.values()) * self.neq * FACE_CELLS * 8
+        return sum(len(v) for v in self.plan.send.values()) * self.neq * 4096 * 8
+
     def dtmin(self) -> float:
         v = ctypes.c_double()
         _lib.check(self.w.lib.wx3d_get_dtmin(self.w.ctx, ctypes.byref(v)), "wx3d_get_dtmin", self.w.ctx)
@@ -172,10 +209,12 @@ class Rank:
 
 class LocalGroup:
     """Transport for several ranks in one process on one device: the halo
-    blocks move by device-to-device copies through a staging buffer."""
+    face slabs (or, with faces=False, whole blocks) move by device-to-device
+    copies through a staging buffer."""
 
-    def __init__(self, ranks):
+    def __init__(self, ranks, faces: bool = True):
         self.ranks = ranks
+        self.faces = faces
 
     def step(self):
         import torch
@@ -196,10 +235,16 @@ class LocalGroup:
     def _exchange(self, array: int):
         import torch
         for src in self.ranks:
-            for peer, bids in src.plan.send.items():
-                buf = torch.empty(len(bids) * src.neq * 4096, dtype=torch.float64, device="cuda")
-                src.pack(array, bids, buf)
-                self.ranks[peer].unpack(array, bids, buf)
+            if self.faces:
+                for peer, items in src.plan.send_faces.items():
+                    buf = torch.empty(len(items) * src.neq * FACE_CELLS, dtype=torch.float64, device="cuda")
+                    src.pack_faces(array, items, buf)
+                    self.ranks[peer].unpack_faces(array, items, buf)
+            else:
+                for peer, bids in src.plan.send.items():
+                    buf = torch.empty(len(bids) * src.neq * 4096, dtype=torch.float64, device="cuda")
+                    src.pack(array, bids, buf)
+                    self.ranks[peer].unpack(array, bids, buf)
 
     def gather(self) -> dict:
         out = {}
@@ -213,11 +258,13 @@ class LocalGroup:
 class TorchDist:
     """Transport between processes through torch.distributed (NCCL between
     GPUs): all_reduce(MIN) of the CFL minimum, batched isend/irecv of the
-    halo blocks in device buffers."""
+    halo face slabs (or, with faces=False, whole blocks) in device
+    buffers."""
 
-    def __init__(self, rank: Rank, device="cuda"):
+    def __init__(self, rank: Rank, device="cuda", faces: bool = True):
         self.r = rank
         self.device = device
+        self.faces = faces
 
     def step(self):
         import torch
@@ -235,24 +282,28 @@ class TorchDist:
     def exchange(self, array: int):
         import torch
         import torch.distributed as dist
-        n = self.r.neq * 4096
+        plan = self.r.plan
+        send, recv = (plan.send_faces, plan.recv_faces) if self.faces else (plan.send, plan.recv)
+        n = self.r.neq * (FACE_CELLS if self.faces else 4096)
+        pack = self.r.pack_faces if self.faces else self.r.pack
+        unpack = self.r.unpack_faces if self.faces else self.r.unpack
         ops, sends, recvs = [], [], []
-        for peer in sorted(set(self.r.plan.send) | set(self.r.plan.recv)):
-            if peer in self.r.plan.send:
-                bids = self.r.plan.send[peer]
-                buf = torch.empty(len(bids) * n, dtype=torch.float64, device=self.device)
-                self.r.pack(array, bids, buf)
+        for peer in sorted(set(send) | set(recv)):
+            if peer in send:
+                items = send[peer]
+                buf = torch.empty(len(items) * n, dtype=torch.float64, device=self.device)
+                pack(array, items, buf)
                 sends.append(buf)
                 ops.append(dist.P2POp(dist.isend, buf, peer))
-            if peer in self.r.plan.recv:
-                bids = self.r.plan.recv[peer]
-                buf = torch.empty(len(bids) * n, dtype=torch.float64, device=self.device)
-                recvs.append((bids, buf))
+            if peer in recv:
+                items = recv[peer]
+                buf = torch.empty(len(items) * n, dtype=torch.float64, device=self.device)
+                recvs.append((items, buf))
                 ops.append(dist.P2POp(dist.irecv, buf, peer))
         if ops:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
         if str(self.device).startswith("cuda"):
             torch.cuda.synchronize()
-        for bids, buf in recvs:
-            self.r.unpack(array, bids, buf)
+        for items, buf in recvs:
+            unpack(array, items, buf)
