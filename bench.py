@@ -160,10 +160,10 @@ def fp64_peak_tflops(lib):
 
 
 def run_reference(args, rank, world):
+    if rank != 0:   # one CPU run per job: the other ranks exit without work
+        return
     prob = build_problem(args.workload)
     threads = os.cpu_count() or 1
-    if rank != 0:
-        return
     budget = float(os.environ.get("WX3D_REF_BUDGET_S", "90"))
     # warm-up steps are whole oracle steps too, bounded by a share of the budget
     import oracle
