@@ -40,8 +40,10 @@ WORKLOADS = {
     "brio-wu": dict(desc="Brio-Wu MHD shock tube 256x16x16 cells, FP64 HLLD+minmod, 8-wave source"),
     "snr-h": dict(desc="radiative SNR, H-rate EOS + COOL_H, 8^3 roots, 4 levels (4,712 blocks), FP64 HLLC+minmod"),
     "winds": dict(desc="colliding stellar winds: 2 sources re-imposed every stage, EOS_H_RATE + 200-row "
-                       "COOL_TABLE, 8^3 roots, 6 levels (19,720 blocks), FP64 HLLC+minmod"),
+                       "COOL_TABLE, 8^3 roots, 6 levels (20,896 blocks), FP64 HLLC+minmod"),
     "snr-h-small": dict(desc="radiative SNR, H-rate EOS + COOL_H, 8^3 roots, 3 levels (1,184 blocks), FP64 HLLC+minmod"),
+    "snr-h-c4": dict(desc="radiative SNR, H-rate EOS + COOL_H, 4^3 roots (64^3 root cells), 4 levels (960 blocks), "
+                          "FP64 HLLC+minmod"),
 }
 
 
@@ -59,6 +61,8 @@ def build_problem(name: str):
         return problems.snr_h(nroot=8, maxlev=4)
     if name == "snr-h-small":
         return problems.snr_h(nroot=8, maxlev=3)
+    if name == "snr-h-c4":
+        return problems.snr_h(nroot=4, maxlev=4)
     if name == "winds":
         return problems.colliding_winds()
     raise SystemExit(f"unknown workload {name}")
