@@ -414,6 +414,13 @@ int wx3d_set_surrogate(wx_ctx* ctx, wx_mlp* mlp, const uint8_t* trust, int32_t n
  * over the n positive normal arguments host_x. */
 int wx3d_check_fast_math(int32_t n, const double* host_x, int64_t* max_ulp2);
 
+/* Self-check of the bounded waits of the tensor-core kernels (no
+ * counterpart in the reference): one CTA waits, giving up after `limit`
+ * tries (1 .. 2^22), on an mbarrier that nothing arrives at, and records the
+ * timeout as the MLP kernels do.  Returns WX_ERR_TIMEOUT, the expected
+ * outcome; the device stays usable. */
+int wx3d_check_wait_timeout(int32_t limit);
+
 /* Measured FP64 FMA throughput of the current device in GFLOP/s (an FMA
  * counts two flops): the compute roofline of the stage kernels. */
 int wx3d_measure_fp64_peak(double* gflops);

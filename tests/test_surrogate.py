@@ -111,3 +111,24 @@ def test_training_reduces_loss():
     assert np.all(np.isfinite(losses))
     l1, _ = s.gradient(x, t)
     assert l1 < l0 / 3.0, (l0, losses, l1)
+
+
+def test_bounded_wait_times_out_and_the_device_stays_usable():
+    """The tensor-core kernels wait on mbarriers with an iteration limit.
+    A wait that nothing ends (an mbarrier no one arrives at) gives up,
+    records the timeout and returns: WX_ERR_TIMEOUT, and the next kernels
+    (a forward pass of the network) run normally."""
+    import torch
+
+    from oracle import mlp_ref
+    from walicxe3d_b200 import _lib
+    from walicxe3d_b200.surrogate import Surrogate
+
+    lib = _lib.load()
+    assert lib.wx3d_check_wait_timeout(4096) == 101
+    assert lib.wx3d_check_wait_timeout(0) == 103
+    s = Surrogate(seed=7)
+    x = _rand_inputs(256)
+    y = s.forward(torch.from_numpy(x).cuda()).cpu().numpy()
+    yr, _ = mlp_ref.forward(s.params.astype(np.float64), x.astype(np.float64), quant=True)
+    assert np.abs(y - yr).max() <= 2e-3 * max(1.0, np.abs(yr).max())

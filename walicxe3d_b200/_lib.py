@@ -86,6 +86,7 @@ _SIGNATURES = {
                                       ctypes.c_float, c_float_p]),
     "wx3d_check_fast_math": (ctypes.c_int, [ctypes.c_int32, c_double_p, ctypes.POINTER(ctypes.c_int64)]),
     "wx3d_measure_fp64_peak": (ctypes.c_int, [c_double_p]),
+    "wx3d_check_wait_timeout": (ctypes.c_int, [ctypes.c_int32]),
     "wx3d_sources": (ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_double)]),
     "wx3d_set_surrogate": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
     "wx3d_error_string": (ctypes.c_char_p, [ctypes.c_int32]),

@@ -118,10 +118,11 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Bounded wait for the phase with the given parity; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait for the phase with the given parity; returns false after
+// `limit` unsuccessful tries (the kernel then records an error and returns).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit = 1 << 22) {
   const uint32_t a = smem_u32(bar);
-  for (int it = 0; it < (1 << 22); ++it) {
+  for (int it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -910,6 +911,17 @@ __global__ void __launch_bounds__(TILE, 4) surrogate_source_kernel(SurrParams P)
   if (t == 0 && s.err) atomicAdd(P.err, 1);
 }
 
+// Waits, with the kernels' bounded wait, on an mbarrier that nothing
+// arrives at, and records the timeout the way the MLP kernels do: the test
+// of the error path that a lost MMA completion would take.
+__global__ void wait_timeout_probe_kernel(int limit, int* err) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  const bool ok = __syncthreads_and(mbar_wait(&bar, 0, limit));
+  if (!ok && threadIdx.x == 0) atomicAdd(err, 1);
+}
+
 }  // namespace mlp
 }  // namespace wx
 
@@ -1061,6 +1073,23 @@ int wx3d_mlp_samples(const wx_config* cfg, int64_t n, uint64_t seed, float* d_in
 }
 
 // Inference with the tcgen05 forward kernel.
+int wx3d_check_wait_timeout(int32_t limit) {
+  if (limit < 1 || limit > (1 << 22)) return WX_ERR_INVALID_ARG;
+  int* err = nullptr;
+  if (cudaMalloc(&err, sizeof(int)) != cudaSuccess) return WX_ERR_CUDA;
+  int e = 0;
+  cudaError_t ce = cudaMemset(err, 0, sizeof(int));
+  if (ce == cudaSuccess) {
+    wait_timeout_probe_kernel<<<1, 128>>>(limit, err);
+    ce = cudaGetLastError();
+  }
+  if (ce == cudaSuccess) ce = cudaDeviceSynchronize();
+  if (ce == cudaSuccess) ce = cudaMemcpy(&e, err, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(err);
+  if (ce != cudaSuccess) return WX_ERR_CUDA;
+  return e ? WX_ERR_TIMEOUT : WX_OK;
+}
+
 int wx3d_mlp_forward(wx_mlp* w, int64_t n, const float* d_in, float* d_out, void* stream) {
   if (!w || n <= 0 || !d_in || !d_out) return WX_ERR_INVALID_ARG;
   const long long ntiles = (n + TILE - 1) / TILE;
