@@ -671,3 +671,14 @@ def test_invalid_meshes_are_refused():
     w.set_state(time=0.0, dt=0.0, it=10, nextout=1)
     w.step()
     assert np.all(np.isfinite(w.download()))
+
+
+@pytest.mark.parametrize("solver", [C.SOLVER_LAX, C.SOLVER_HLL1, C.SOLVER_HLL])
+def test_other_solvers_on_a_three_level_mesh(solver, ncpu):
+    """Lax-Friedrichs (one-deep ghosts of U, lax.f90:39-99), the first-order
+    HLL1 stage, and HLL on the three-level AMR blast: coarse/fine ghost
+    fills under each solver's own stencil, and the zero UP ghosts the
+    single-stage solvers give the viscous step."""
+    prob = small_amr(solver=solver)
+    o, g = run_both(prob, 10, ncpu)
+    check(o, g, prob)
