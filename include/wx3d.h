@@ -166,7 +166,10 @@ int wx3d_set_stream(wx_ctx* ctx, void* cuda_stream);
 
 /* localBlocks registry: bID of the block held in each slot, -1 if empty
  * (source/globals.f90:125, source/init.f90:431-437).  Rebuilds the device
- * neighbour table with the reference's tree queries (source/amr.f90:439-631). */
+ * neighbour table with the reference's tree queries (source/amr.f90:439-631).
+ * Every slot may be -1 (a process that holds no block): the steps then run
+ * no block and the local dt is 1e30*CFL, as getTimestep gives such a
+ * process (source/hydro_solver.f90:145-192); wx3d_autotune needs a block. */
 int wx3d_set_mesh(wx_ctx* ctx, int32_t nslots, const int32_t* local_blocks);
 
 /* A process's share of a partitioned mesh: as wx3d_set_mesh, with nhalo of

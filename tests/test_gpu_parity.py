@@ -673,6 +673,35 @@ def test_invalid_meshes_are_refused():
     assert np.all(np.isfinite(w.download()))
 
 
+@pytest.mark.parametrize("use_run", [False, True])
+def test_an_empty_mesh_steps_like_the_reference(use_run):
+    """A process whose localBlocks are all -1 (more processes than blocks):
+    its loops find no block, its local dt is 1e30*CFL (getTimestep,
+    hydro_solver.f90:145-192), clamped to the next output time, and each step
+    advances time, it and nextout as the oracle's does, through wx3d_step and
+    through the graph replay of wx3d_run."""
+    prob = problems.brio_wu(4)
+    empty = np.full(4, -1, np.int32)
+    o = oracle.Oracle(prob.cfg, 4)
+    o.set_blocks(empty)
+    w = Walicxe3D(prob.cfg, 4)
+    w.set_mesh(empty)
+    for x in (o, w):
+        x.set_state(time=0.0, dt=0.0, it=3, nextout=1)
+    for _ in range(3):
+        o.step()
+    if use_run:
+        w.run(3)
+    else:
+        for _ in range(3):
+            w.step()
+    so, sg = o.state, w.state
+    assert (sg.time, sg.dt, sg.it, sg.nextout) == (so.time, so.dt, so.it, so.nextout)
+    assert so.it == 6 and so.time > 0.0
+    o.close()
+    w.close()
+
+
 @pytest.mark.parametrize("solver", [C.SOLVER_LAX, C.SOLVER_HLL1, C.SOLVER_HLL])
 def test_other_solvers_on_a_three_level_mesh(solver, ncpu):
     """Lax-Friedrichs (one-deep ghosts of U, lax.f90:39-99), the first-order

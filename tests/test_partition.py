@@ -49,6 +49,23 @@ def test_plan_covers_every_neighbour_and_is_symmetric():
                         assert (h, g) in {it for its in p.recv_faces.values() for it in its}
 
 
+def test_more_ranks_than_blocks_leaves_empty_shares():
+    """Six shares of Brio-Wu's four blocks: every block owned exactly once,
+    two shares empty, and an empty share neither sends nor receives."""
+    prob = problems.brio_wu(4)
+    plans = make_plan(prob.local_blocks, prob.cfg.nbroot, prob.cfg.maxlev, 6)
+    owned = [b for p in plans for b in p.owned]
+    assert sorted(owned) == sorted(int(b) for b in prob.local_blocks)
+    empty = [p for p in plans if not p.owned]
+    assert len(empty) == 2
+    for p in empty:
+        assert not p.halo and not p.send and not p.recv and not p.send_faces and not p.recv_faces
+        assert len(p.local_blocks) == 0
+    for p in plans:
+        for q in p.send:
+            assert plans[q].owned
+
+
 def test_face_neighbours_of_a_three_level_mesh_are_levels_apart_by_one():
     prob = _amr()
     tree = BlockTree(prob.cfg.nbroot, prob.cfg.maxlev)
@@ -123,11 +140,13 @@ def test_halo_exchange_between_two_gloo_processes(faces):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,nranks,faces", [("amr", 2, True), ("amr", 3, True), ("snr-h", 2, True),
-                                               ("brio-wu", 2, True), ("amr", 3, False)])
+                                               ("brio-wu", 2, True), ("amr", 3, False),
+                                               ("brio-wu", 6, True)])
 def test_partitioned_step_equals_single_context(name, nranks, faces):
     """Ranks on one device exchanging their halo face slabs (or whole halo
     blocks) reproduce the single-context run bit for bit: same fluxes per
-    block, same global dt."""
+    block, same global dt.  Six ranks over Brio-Wu's four blocks leave two
+    ranks without a block; they still take part in the dt minimum."""
     from walicxe3d_b200.partition import LocalGroup, Rank
     from walicxe3d_b200.solver import from_problem
     prob = {"amr": _amr, "snr-h": lambda: problems.snr_h(nroot=2, maxlev=2),

@@ -235,6 +235,7 @@ struct wx_ctx {
   std::vector<double> hwind;      // wind sources, 12 doubles each (wx_wind)
   double* dWind = nullptr;
   int nwork = 0;
+  bool mesh_set = false;  // a mesh was set; it may hold no blocks (localBlocks all -1)
   int zsplit = 1;
   bool fuse = true;   // corrector carries the viscous step when zsplit == 1
   int zero_ghost = 0; // single-stage solver: the viscous step sees zero UP ghosts
@@ -607,7 +608,10 @@ void invalidate_graph(wx_ctx* c) {
   c->graph_valid = false;
 }
 
-bool ready(wx_ctx* c) { return c && c->nwork > 0; }
+// A process whose localBlocks are all -1 still steps: its loops find no
+// block, its local dt is 1e30*CFL and time advances with the others
+// (getTimestep, hydro_solver.f90:145-205).
+bool ready(wx_ctx* c) { return c && c->mesh_set; }
 
 // FP64 FMA throughput: 8 independent chains per thread, 4096 steps each.
 __global__ void __launch_bounds__(256) fp64_peak_kernel(double* out, double a, double b) {
@@ -883,6 +887,7 @@ int wx3d_set_mesh_halo(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nha
   std::swap(c->hblocks, c->hblocks_next);
   c->work = std::move(work);
   c->nwork = (int)c->work.size();
+  c->mesh_set = true;
   WX_CUDA(cudaMemcpyAsync(c->dBlocks, c->hblocks, sizeof(DevBlock) * c->max_blocks, cudaMemcpyHostToDevice, c->stream));
   if (!c->work.empty())
     WX_CUDA(cudaMemcpyAsync(c->dWork, c->work.data(), 4 * c->work.size(), cudaMemcpyHostToDevice, c->stream));
@@ -1063,7 +1068,7 @@ int wx3d_set_fusion(wx_ctx* c, int32_t on) {
 }
 
 int wx3d_autotune(wx_ctx* c, int32_t reps, double* ms5, int32_t* best) {
-  if (!ready(c) || reps <= 0) return WX_ERR_INVALID_ARG;
+  if (!ready(c) || c->nwork == 0 || reps <= 0) return WX_ERR_INVALID_ARG;
   if (c->cfg.solver_type == WX_SOLVER_LAX) {
     if (best) { best[0] = 1; best[1] = 0; }
     return WX_OK;
@@ -1129,7 +1134,8 @@ int wx3d_get_neighbours(wx_ctx* c, int32_t nslots, int32_t* ft, int32_t* fs) {
 
 int wx3d_upload_blocks(wx_ctx* c, int32_t nslots, const double* u) {
   if (!c || !u || nslots < 0 || nslots > c->max_blocks) return WX_ERR_INVALID_ARG;
-  WX_CUDA(cudaMemcpyAsync(c->dU, u, (size_t)nslots * c->neq * BCELLS * 8, cudaMemcpyHostToDevice, c->stream));
+  if (nslots > 0)
+    WX_CUDA(cudaMemcpyAsync(c->dU, u, (size_t)nslots * c->neq * BCELLS * 8, cudaMemcpyHostToDevice, c->stream));
   WX_CUDA(cudaStreamSynchronize(c->stream));
   c->dt_valid = false;
   c->prestep = false;
@@ -1138,7 +1144,8 @@ int wx3d_upload_blocks(wx_ctx* c, int32_t nslots, const double* u) {
 
 int wx3d_download_blocks(wx_ctx* c, int32_t nslots, double* u) {
   if (!c || !u || nslots < 0 || nslots > c->max_blocks) return WX_ERR_INVALID_ARG;
-  WX_CUDA(cudaMemcpyAsync(u, c->dU, (size_t)nslots * c->neq * BCELLS * 8, cudaMemcpyDeviceToHost, c->stream));
+  if (nslots > 0)
+    WX_CUDA(cudaMemcpyAsync(u, c->dU, (size_t)nslots * c->neq * BCELLS * 8, cudaMemcpyDeviceToHost, c->stream));
   WX_CUDA(cudaStreamSynchronize(c->stream));
   return WX_OK;
 }

@@ -949,6 +949,7 @@ cudaError_t launch_surrogate_source(const SurrLaunch& L, cudaStream_t s) {
   SurrParams P{L.u,      L.blocks,  L.work,    L.nwork,      L.ctl,       L.ph,     L.mlp->pk, L.mlp->prm,
                L.trust,  L.do_dt,   L.mlp->err, L.cool_lt,   L.cool_lc,   L.ncool,  L.nZ};
   const long long ntiles = (long long)L.nwork * (BCELLS / TILE);
+  if (ntiles == 0) return cudaSuccess;  // no local block
   const int grid = (int)std::min<long long>(ntiles, 4LL * L.nsm);
   if (L.neq == 6) {
     cudaFuncSetAttribute(surrogate_source_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INF_SMEM);

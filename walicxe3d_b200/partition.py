@@ -133,7 +133,9 @@ class Rank:
         self.plan = plan
         self.prob = prob
         lb = plan.local_blocks
-        self.w = Walicxe3D(prob.cfg, len(lb))
+        # with more ranks than blocks a share is empty: the rank still takes
+        # part in the dt minimum, like a process whose localBlocks are all -1
+        self.w = Walicxe3D(prob.cfg, max(1, len(lb)))
         if stream_handle is not None:
             self.w.set_stream(stream_handle)
         nh = len(plan.halo)
