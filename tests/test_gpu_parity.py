@@ -336,6 +336,20 @@ def test_sedov_256_conservation_and_symmetry():
     assert np.abs(G - G.transpose(2, 1, 0)).max() <= 1e-12 * scale
 
 
+def test_blast_amr_full_size_matches_oracle(ncpu):
+    """The benchmark's headline mesh at full size (8^3 roots, 5 levels,
+    11,600 blocks, 47.5M cells), stepped through the replayed CUDA graph of
+    wx3d_run with the launch shape the mesh size selects (whole blocks, the
+    viscous step fused into the corrector), against the oracle over all
+    blocks."""
+    prob = problems.blast_amr()
+    assert prob.nblocks == 11600
+    o, g = run_both(prob, 3, ncpu, use_run=True)
+    check(o, g, prob)
+    g.close()
+    o.close()
+
+
 def test_status_counts_and_zero_density_error():
     prob = problems.sedov(2)
     U = prob.U.copy()
