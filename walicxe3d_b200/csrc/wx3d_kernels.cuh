@@ -1,6 +1,6 @@
 // wx3d_kernels.cuh -- sm_100a kernels of the per-block Godunov update.
 //
-// Stage kernel: one CTA per (block, z-slab).  288 threads (9 warps) march
+// Stage kernel: one CTA per (block, z-slab).  320 threads (10 warps) march
 // through the slab's k-planes; a 4-plane shared-memory ring holds the
 // primitives of each plane together with its two-deep x/y ghost frame, so
 // every x-, y- and z-interface flux is computed exactly once and the
@@ -13,7 +13,12 @@
 
 namespace wx {
 
-constexpr int STAGE_THREADS = 288;  // 17*16 x- and y-interfaces per plane
+// 17*16 x- and y-interfaces per plane on the first 272 threads; the plane
+// loads (320 cells at first order, 384 at second) spread over all 320, and
+// two CTAs per SM put five warps on every sub-partition
+constexpr int STAGE_THREADS = 320;
+static_assert(STAGE_THREADS >= 17 * NC, "one thread per x- and y-interface of a plane");
+static_assert(STAGE_THREADS >= PLANE + 4 * NC, "the viscous step's UP frame is gathered by threads PLANE..PLANE+63");
 constexpr int RING = 4;             // planes p-1..p+2 of the second-order stencil
 
 struct StageParams {
@@ -226,7 +231,7 @@ __device__ __forceinline__ void load_plane(const StageParams& P, const DevBlock&
 // the buffer slot that W(m) replaces, read first by the same thread) and
 // W(m) (in registers).  The block-face z-neighbours are UP ghosts as well.
 // Two CTAs per SM where the shared memory allows it; registers are then
-// capped at 96 per thread (nine warps per CTA, five on one sub-partition).
+// capped at 96 per thread (ten warps per CTA, five on each sub-partition).
 template <int NEQ, bool MHD, int ORDER, bool VISC>
 __host__ __device__ constexpr int stage_ctas_per_sm() {
   return (!MHD && 2 * (stage_smem_bytes<NEQ, MHD, ORDER, VISC>() + 1024) <= 228 * 1024) ? 2 : 1;
@@ -307,11 +312,11 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
     for (int m = z0; m <= z1; ++m) {
       // ---- phase A: load plane m+ORDER+1; z-flux m+1/2; x/y fluxes of m ---
       if (m + ORDER + 1 <= z1 + ORDER) load_plane<NEQ, MHD, ORDER, CH>(P, B, slot, m + ORDER + 1, z0, z1, ring, pf, df, zd);
-      // one-deep x/y frame of W(m): UP ghosts of plane m, on threads 96..159,
-      // which load a single ring cell per plane (threads below 96 load two)
-      if (VISC && t >= 96 && t < 96 + 4 * NC) {
+      // one-deep x/y frame of W(m): UP ghosts of plane m, on threads 256..319,
+      // which compute no z-flux and at most one x/y interface pair
+      if (VISC && t >= PLANE && t < PLANE + 4 * NC) {
         {
-          const int f = t - 96;
+          const int f = t - PLANE;
           const int side = f >> 4, r = (f & 15) + 1;
           const int gi = side == 0 ? 0 : (side == 1 ? NC + 1 : r);
           const int gj = side == 2 ? 0 : (side == 3 ? NC + 1 : r);
