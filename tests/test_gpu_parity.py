@@ -464,6 +464,31 @@ def test_wind_sphere_on_a_level_transition_is_refused():
     g.step()   # the previous sources stay in force
 
 
+def test_mesh_refused_for_a_wind_sphere_keeps_the_previous_mesh(tmp_path):
+    """wx3d_set_mesh refusing a mesh with a coarse/fine face through a wind
+    sphere (one level-2 block at the first source refined, its neighbours
+    not) keeps the previous mesh whole, its slot registry included: a
+    checkpoint written afterwards carries the previous mesh's bIDs."""
+    from walicxe3d_b200._lib import WxError
+    prob = problems.colliding_winds(nroot=2, maxlev=3, r_wind_cells=8)
+    g = from_problem(prob)
+    t = BlockTree(prob.cfg.nbroot, 3).roots()
+    for b in sorted(t.leaves):
+        t.refine(b)
+    src = np.array([0.25, 0.5, 0.5]) + 1e-3          # just inside the block cornered at the first source
+    inside = [b for b in t.leaves if np.all(t.bounds(b)[0] <= src) and np.all(src < t.bounds(b)[1])]
+    assert len(inside) == 1
+    t.refine(inside[0])
+    with pytest.raises(WxError) as e:
+        g.set_mesh(np.array(sorted(t.leaves), np.int32))
+    assert e.value.code == 104
+    g.write_bin(tmp_path / "b.bin")
+    h = Walicxe3D(prob.cfg, g.max_blocks)
+    lb = h.read_bin(tmp_path / "b.bin")
+    assert sorted(int(b) for b in lb if b != -1) == sorted(int(b) for b in prob.local_blocks)
+    g.step()
+
+
 def test_small_wind_sphere_fails_at_the_same_step_as_the_reference(ncpu):
     """With wind spheres of 8 finest cells the reference algorithm goes
     non-finite next to the strong source at the end of the dt ramp; the GPU

@@ -877,13 +877,14 @@ int wx3d_set_mesh_halo(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nha
     }
     if (lb[s] != -1 && !is_halo[s]) work.push_back(s);
   }
-  c->local.assign(c->max_blocks, -1);
-  std::copy(lb, lb + nslots, c->local.begin());
-  c->nhalo = nhalo;
   int bad = -1;
   if (!flag_wind_blocks(c, hb, c->max_blocks, &bad))
     return fail(c, WX_ERR_UNSUPPORTED, "slot %d: a wind sphere reaches the ghost layer of a coarse/fine face; "
                 "refine the zone around the source (refineZone) further", bad);
+  // accepted: from here on the context holds the new mesh
+  c->local.assign(c->max_blocks, -1);
+  std::copy(lb, lb + nslots, c->local.begin());
+  c->nhalo = nhalo;
   std::swap(c->hblocks, c->hblocks_next);
   c->work = std::move(work);
   c->nwork = (int)c->work.size();
