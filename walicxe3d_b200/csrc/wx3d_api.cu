@@ -784,7 +784,11 @@ int wx3d_set_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb) { return wx3d_se
 // As wx3d_set_mesh, with nhalo slots holding copies of blocks another
 // process owns: they are read as neighbours but never updated, and their
 // own faces may lead out of the local block set.
-int wx3d_set_mesh_halo(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nhalo, const int32_t* halo) {
+// Builds the neighbour table of a mesh into hblocks_next and its work list,
+// refusing what the tree queries cannot resolve and wind spheres on a
+// coarse/fine face; the context's mesh and state are left as they are.
+static int build_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nhalo, const int32_t* halo,
+                      std::vector<int32_t>& work) {
   if (!c || !lb || nslots < 0 || nhalo < 0 || (nhalo > 0 && !halo)) return WX_ERR_INVALID_ARG;
   std::vector<char> is_halo(c->max_blocks, 0);
   for (int h = 0; h < nhalo; ++h) {
@@ -867,7 +871,7 @@ int wx3d_set_mesh_halo(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nha
   };
 #pragma omp parallel for schedule(dynamic, 512) if (nslots > 4096)
   for (int s = 0; s < nslots; ++s) face_err[s] = entry(s);
-  std::vector<int32_t> work;
+  work.clear();
   work.reserve(nslots);
   for (int s = 0; s < nslots; ++s) {
     if (face_err[s]) {
@@ -881,7 +885,11 @@ int wx3d_set_mesh_halo(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nha
   if (!flag_wind_blocks(c, hb, c->max_blocks, &bad))
     return fail(c, WX_ERR_UNSUPPORTED, "slot %d: a wind sphere reaches the ghost layer of a coarse/fine face; "
                 "refine the zone around the source (refineZone) further", bad);
-  // accepted: from here on the context holds the new mesh
+  return WX_OK;
+}
+
+// Makes the mesh that build_mesh left in hblocks_next the context's.
+static int commit_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nhalo, std::vector<int32_t>& work) {
   c->local.assign(c->max_blocks, -1);
   std::copy(lb, lb + nslots, c->local.begin());
   c->nhalo = nhalo;
@@ -900,6 +908,12 @@ int wx3d_set_mesh_halo(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nha
   c->prestep = false;
   invalidate_graph(c);
   return WX_OK;
+}
+
+int wx3d_set_mesh_halo(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nhalo, const int32_t* halo) {
+  std::vector<int32_t> work;
+  const int rc = build_mesh(c, nslots, lb, nhalo, halo, work);
+  return rc ? rc : commit_mesh(c, nslots, lb, nhalo, work);
 }
 
 int wx3d_set_zsplit(wx_ctx* c, int32_t zsplit) {
@@ -1806,6 +1820,10 @@ int wx3d_admesh(wx_ctx* c, int32_t nbmax, int32_t* lb, int32_t* counts) {
     counts[1] = ncoarse;
   }
   if (rops.empty() && cops.empty()) return WX_OK;  // the mesh and the state stay as they are
+  // the new mesh is checked before any data moves, so a refused mesh
+  // leaves the state and the slot registry as they were
+  std::vector<int32_t> work;
+  if ((rc = build_mesh(c, nbmax, L.lb.data(), 0, nullptr, work))) return rc;
   // data: refinements, then coarsenings.  Each pass first copies the blocks
   // it reads (fathers, or siblings) from U into UP at the same slots -- UP
   // holds nothing between steps, the next predictor overwrites it -- then
@@ -1833,7 +1851,7 @@ int wx3d_admesh(wx_ctx* c, int32_t nbmax, int32_t* lb, int32_t* counts) {
     }
   }
   const int zsplit = c->zsplit;  // the launch shape chosen for the context stays
-  if ((rc = wx3d_set_mesh(c, nbmax, L.lb.data()))) return rc;
+  if ((rc = commit_mesh(c, nbmax, L.lb.data(), 0, work))) return rc;
   c->zsplit = zsplit;
   std::copy(L.lb.begin(), L.lb.end(), lb);
   return WX_OK;
