@@ -133,7 +133,7 @@ def train(n_train: int, n_test: int, out: str, seed: int = 1, batch: int = 16384
     t_samples = time.time() - t0
     s = Surrogate(seed=seed)
 
-    def judge(xs, ts, rs):
+    def evaluate(xs, ts, rs):
         pred = s.forward(xs).cpu().numpy()
         raw = rs.cpu().numpy()
         ex, eT = errors(pred, ts.cpu().numpy(), raw)
@@ -148,7 +148,7 @@ def train(n_train: int, n_test: int, out: str, seed: int = 1, batch: int = 16384
     rb = _bins_device(r)
     del r
     for factor, sched in SCHEDULE_FOCUS:
-        ex, eT, b = judge(xt, tt, rt)
+        ex, eT, b = evaluate(xt, tt, rt)
         cnt, mx, mt = bin_max(ex, eT, b)
         dropped |= (mx > factor * X_TOL) | (mt > factor * T_TOL)
         keep = ~torch.from_numpy(dropped).to(x.device)[rb]
@@ -160,10 +160,10 @@ def train(n_train: int, n_test: int, out: str, seed: int = 1, batch: int = 16384
     torch.cuda.synchronize()
     t_train = time.time() - t0
 
-    ex, eT, b = judge(xt, tt, rt)
+    ex, eT, b = evaluate(xt, tt, rt)
     table = trust_table(ex, eT, b, margin=TRUST_MARGIN)
     cnt, mx, mt = bin_max(ex, eT, b)
-    exv, eTv, bv = judge(xv, tv, rv)
+    exv, eTv, bv = evaluate(xv, tv, rv)
     inside = table[bv] != 0
     stats = {
         "n_train": n_train,
