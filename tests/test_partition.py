@@ -82,6 +82,17 @@ class _CpuRank:
         self.plan, self.neq = plan, neq
         self.data = {b: torch.full((neq * 4096,), float(values[b])) for b in plan.owned}
         self.data.update({b: torch.zeros(neq * 4096) for b in plan.halo})
+        self.vals = [float(values[b]) for b in plan.owned]
+        self.dt = None
+
+    def dtmin(self):
+        return min(self.vals, default=1.0e30)   # no block: getTimestep's 1e30
+
+    def set_dtmin(self, v):
+        self.dt = v
+
+    def part(self, p):
+        pass
 
     def pack(self, array, bids, buf):
         buf.copy_(torch.cat([self.data[b] for b in bids]))
@@ -136,6 +147,44 @@ def test_halo_exchange_between_two_gloo_processes(faces):
     for p in procs:
         p.join(timeout=60)
     assert all(ok and nh > 0 and m == 1.0 for _, ok, nh, m in res), res
+
+
+def _step_worker(rank, world, port, q):
+    import torch.distributed as dist
+    from walicxe3d_b200.partition import TorchDist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        prob = problems.brio_wu(2)
+        plans = make_plan(prob.local_blocks, prob.cfg.nbroot, prob.cfg.maxlev, world)
+        values = {int(b): 10.0 + float(b) for b in prob.local_blocks}
+        r = _CpuRank(plans[rank], 2, values)
+        TorchDist(r, device="cpu", faces=True).step()
+        items = [it for its in plans[rank].recv_faces.values() for it in its]
+        ok = all(bool(torch.all(r.data[(b, f)] == values[b])) for b, f in items)
+        q.put((rank, ok, len(plans[rank].owned), len(items), r.dt))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_step_choreography_with_an_empty_rank_over_gloo():
+    """Three gloo processes over Brio-Wu's two blocks: the middle rank owns
+    nothing, contributes getTimestep's 1e30 to the dt minimum, sends and
+    receives no slab, and the step completes on every rank with the same
+    dt; the two other ranks receive each other's face slab."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_step_worker, args=(r, 3, 29615, q)) for r in range(3)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+    assert [n for _, _, n, _, _ in res] == [1, 0, 1]
+    assert [k for _, _, _, k, _ in res] == [1, 0, 1]
+    assert all(ok for _, ok, _, _, _ in res)
+    assert all(dt == 11.0 for *_, dt in res)
 
 
 @pytest.mark.gpu
