@@ -171,3 +171,22 @@ def test_admesh_keeps_mass_balance_and_cover(ncpu):
             for n in face_neighbours(tree, leaves, b):
                 assert abs(tree.level(n) - tree.level(b)) <= 1
     assert total[0] >= 5 and total[1] >= 5
+
+
+def test_a_process_without_blocks_takes_the_output_clamped_dt():
+    """getTimestep (hydro_solver.f90:145-205) on a process whose localBlocks
+    are all -1: dt_loc = 1e30*CFL (halved per boot-up step), so the clamp to
+    the next output time, nextout*dtout/t_sc - time, decides dt; the step
+    then reaches the output time."""
+    prob = problems.brio_wu(4)
+    o = oracle.Oracle(prob.cfg, 4)
+    o.set_blocks(np.full(4, -1, np.int32))
+    want = prob.cfg.dtout / prob.cfg.t_sc
+    for it in (0, 10, 11):
+        o.set_state(time=0.0, dt=0.0, it=it, nextout=1)
+        assert o.get_timestep() == want
+    o.set_state(time=0.0, dt=0.0, it=3, nextout=1)
+    o.step()
+    s = o.state
+    assert (s.time, s.dt, s.it, s.nextout) == (want, want, 4, 2)
+    o.close()
