@@ -333,8 +333,10 @@ int wx3d_coarsen(wx_ctx* ctx, const int32_t* child_slots8, int32_t father_slot);
  * rebuilt from it (the context's z-slab split is kept); otherwise nothing
  * but the marking runs.
  * counts2 (may be NULL): blocks refined, families coarsened.  Capacity
- * errors (WX_ERR_INSUFICIENT_NBMAXPROC, WX_ERR_REGISTER_FATHER) are found
- * before any data moves and leave the mesh and the state unchanged. */
+ * errors (WX_ERR_INSUFICIENT_NBMAXPROC, WX_ERR_REGISTER_FATHER) and a new
+ * mesh that wx3d_set_mesh would refuse (WX_ERR_MESH, or WX_ERR_UNSUPPORTED
+ * for a wind sphere on a coarse/fine face) are found before any data moves
+ * and leave the mesh and the state unchanged. */
 int wx3d_admesh(wx_ctx* ctx, int32_t nbmax, int32_t* local_blocks, int32_t* counts2);
 
 /* Per-kernel device timing with CUDA events recorded around each launch of
