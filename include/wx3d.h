@@ -355,19 +355,26 @@ int wx3d_reset_status(wx_ctx* ctx);
  * belongs to their own pool or framework allocator, or that must not grow
  * their footprint after start-up.  The caller passes the state in its own
  * device memory: u_in and u_out are [slot][eq][k][j][i] arrays of nslots
- * blocks that must not overlap, local_blocks is the host-side bID
- * registry, *state (host) is read and updated like wx3d_step's.  One
- * main-loop step without source terms is run (it += 1, getTimestep,
- * Godunov / Lax-Friedrichs, viscous step) on cuda_stream (NULL = default
- * stream) and the call returns after the stream is synchronised.
+ * blocks whose byte ranges must not overlap (an overlap returns
+ * WX_ERR_INVALID_ARG), local_blocks is the host-side bID registry, and
+ * *state (host) carries time, dt, it and nextout in and out like
+ * wx3d_step's: on return dumpout reports whether this step crossed an
+ * output time (nextout has then been advanced); its value on entry is
+ * ignored.  One main-loop step without source terms is run (it += 1,
+ * getTimestep, Godunov / Lax-Friedrichs, viscous step) on cuda_stream
+ * (NULL = default stream) and the call returns after the stream is
+ * synchronised.  A registry with no block (all -1) steps like wx3d_step on
+ * an empty mesh: dt = 1e30*CFL clamped to the next output time.
  * Scratch (predictor state, neighbour table, control block) lives in one
  * fixed device array of the library: nslots x neqtot must not exceed
  * WX3D_NOALLOC_MAX_BLOCK_EQS (10 MiB of predictor state), otherwise the call
- * returns WX_ERR_INSUFICIENT_NBMAXPROC.  The first call on each device looks
- * the array up (cudaGetSymbolAddress) and should come before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race
- * and must be serialised by the caller.  Source terms (EOS_H_RATE, cooling)
- * return WX_ERR_UNSUPPORTED. */
+ * returns WX_ERR_INSUFICIENT_NBMAXPROC.  The array's device address is
+ * looked up (cudaGetSymbolAddress) on the first call on each device and
+ * again whenever the current CUDA context changes, so the first call, and
+ * the first after a context change, should come before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  Source terms (EOS_H_RATE, cooling) return
+ * WX_ERR_UNSUPPORTED. */
 #define WX3D_NOALLOC_MAX_BLOCK_EQS 320
 int wx3d_hydro_step_noalloc(const wx_config* cfg, int32_t nslots, const int32_t* local_blocks,
                             const double* u_in, double* u_out, wx_state* state, void* cuda_stream);

@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <mutex>
 #include <queue>
 #include <string>
 #include <unordered_map>
@@ -2033,23 +2034,57 @@ constexpr size_t NOALLOC_BYTES = NOALLOC_CTL_OFF + ((sizeof(DevCtl) + 255) / 256
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 
-// Device address of g_noalloc_scratch per device, looked up once per device
-// with that device current (the symbol is a host-side stand-in in host code).
+// Device address of g_noalloc_scratch (the symbol is a host-side stand-in in
+// host code).  It is looked up with cudaGetSymbolAddress, with the device
+// current, on the first call on a device, and again whenever the current
+// driver context differs from the one the cached address belongs to: a
+// primary context that was reset and recreated, or a caller's own driver-API
+// context, loads the module at another address.  The cache is guarded by a
+// mutex, so host threads making their first calls together are safe (their
+// GPU work still shares the array, see above).
 constexpr int NOALLOC_MAX_DEVICES = 64;
-unsigned char* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+struct NoallocAddr {
+  void* ctx = nullptr;          // driver context the address belongs to (nullptr: unknown)
+  unsigned char* ptr = nullptr;
+};
+std::mutex g_noalloc_mu;
+NoallocAddr g_noalloc_addr[NOALLOC_MAX_DEVICES];
+
+// The current driver context (CUcontext), through the runtime's driver entry
+// point so the library needs no link against libcuda; nullptr when it cannot
+// be told, in which case the address is looked up on every call.
+void* noalloc_current_context() {
+  using CtxGetCurrent = int (*)(void**);
+  static const CtxGetCurrent fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<CtxGetCurrent>(p);
+  }();
+  void* ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
 
 int noalloc_scratch(int dev, unsigned char** out) {
   if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return WX_ERR_INVALID_ARG;
-  if (!g_noalloc_ptr[dev]) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoallocAddr& a = g_noalloc_addr[dev];
+  void* ctx = noalloc_current_context();
+  if (!a.ptr || !ctx || ctx != a.ctx) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
+      a = NoallocAddr{};
       std::fprintf(stderr, "wx3d_hydro_step_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
       return WX_ERR_CUDA;
     }
-    g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    a.ptr = static_cast<unsigned char*>(p);
+    a.ctx = noalloc_current_context();  // the lookup may have made the primary context current
   }
-  *out = g_noalloc_ptr[dev];
+  *out = a.ptr;
   return WX_OK;
 }
 
@@ -2175,6 +2210,16 @@ extern "C" int wx3d_hydro_step_noalloc(const wx_config* cfg, int32_t nslots, con
                  nslots, cfg->neqtot, NOALLOC_MAX_BLOCK_EQS, NOALLOC_MAX_BLOCKS);
     return WX_ERR_INSUFICIENT_NBMAXPROC;
   }
+  {
+    // u_in is read by every stage while u_out is written: the two ranges must
+    // be disjoint (an aliased Lax-Friedrichs or HLL1 step would race)
+    const size_t bytes = (size_t)nslots * cfg->neqtot * BCELLS * sizeof(double);
+    const uintptr_t a0 = reinterpret_cast<uintptr_t>(u_in), b0 = reinterpret_cast<uintptr_t>(u_out);
+    if (a0 < b0 + bytes && b0 < a0 + bytes) {
+      std::fprintf(stderr, "wx3d_hydro_step_noalloc: u_in and u_out overlap\n");
+      return WX_ERR_INVALID_ARG;
+    }
+  }
   Kern k;
   if (!select_kern(*cfg, k)) return WX_ERR_UNSUPPORTED;
   int dev = 0, nsm = 148;
@@ -2194,7 +2239,9 @@ extern "C" int wx3d_hydro_step_noalloc(const wx_config* cfg, int32_t nslots, con
     std::fprintf(stderr, "wx3d_hydro_step_noalloc: invalid mesh\n");
     return rc;
   }
-  if (nwork == 0) return WX_ERR_MESH;
+  // An empty registry steps like wx3d_step on an empty mesh: no block is
+  // updated, the local dt is 1e30*CFL (clamped to the next output time) and
+  // time advances.
   int zsplit = 1;
   while (zsplit < 8 && nwork * zsplit < 2 * nsm) zsplit *= 2;
 
@@ -2205,7 +2252,10 @@ extern "C" int wx3d_hydro_step_noalloc(const wx_config* cfg, int32_t nslots, con
   h.dt = state->dt;
   h.it = state->it;
   h.nextout = state->nextout;
-  h.dumpout = state->dumpout;
+  // The output bookkeeping of a crossed output time finishes inside the call
+  // (step_end_kernel advances nextout), so no pending flag carries over:
+  // state->dumpout on entry is ignored, on return it reports a crossing.
+  h.dumpout = 0;
   const double big = 1.0e30;
   std::memcpy(&h.dtmin_bits, &big, 8);
 

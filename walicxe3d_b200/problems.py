@@ -166,16 +166,17 @@ def orszag_tang_3d(nroot: int = 2, flux_cd: bool = True, solver=C.SOLVER_HLLD, s
 
 
 def amr_pulse(nroot: int = 2, maxlev: int = 3, centre=(0.15, 0.15, 0.15), width: float = 0.03,
-              amplitude: float = 10.0, steps: int = 20) -> Problem:
+              amplitude: float = 10.0, steps: int = 20, refine_roots=None) -> Problem:
     """Live-mesh test: a Gaussian pressure and density pulse in one corner of
     a uniform medium at rest (rho = p = 1), on nroot^3 root blocks all
-    refined once (level 2).  The first admesh coarsens the quiet families and
-    refines the blocks around the pulse; as the pulse spreads, refinement
-    follows it.  HLLC + minmod, CFL 0.4, eta 5e-3, free-flow boundaries."""
+    refined once (level 2), or only the roots listed in refine_roots (bIDs).
+    The first admesh coarsens the quiet families and refines the blocks
+    around the pulse; as the pulse spreads, refinement follows it.  HLLC +
+    minmod, CFL 0.4, eta 5e-3, free-flow boundaries."""
     cfg = Config(solver_type=C.SOLVER_HLLC, limiter_type=C.LIMITER_MINMOD, nbroot=(nroot,) * 3, maxlev=maxlev,
                  gamma=5.0 / 3.0, cfl=0.4, visc_eta=5.0e-3)
     tree = BlockTree(cfg.nbroot, maxlev).roots()
-    for b in sorted(tree.leaves):
+    for b in sorted(tree.leaves) if refine_roots is None else list(refine_roots):
         tree.refine(b)
     c = np.array(centre)
 
