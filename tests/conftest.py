@@ -11,6 +11,7 @@ if str(ROOT) not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and libwx3d.so")
+    config.addinivalue_line("markers", "full_size: a benchmark configuration at its stated size (minutes of oracle time)")
 
 
 def gpu_available() -> bool:

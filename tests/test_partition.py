@@ -111,6 +111,15 @@ class _CpuRank:
             self.data[(b, f)] = buf[i * n:(i + 1) * n].clone()
 
 
+def _free_port() -> int:
+    """An ephemeral port the kernel hands out on 127.0.0.1 (released before
+    the ranks bind it), so concurrent test runs do not collide."""
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
 def _exchange_worker(rank, world, port, q, faces):
     import torch.distributed as dist
     from walicxe3d_b200.partition import TorchDist
@@ -139,7 +148,7 @@ def _exchange_worker(rank, world, port, q, faces):
 def test_halo_exchange_between_two_gloo_processes(faces):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    port = 29611 + int(faces)
+    port = _free_port()
     procs = [ctx.Process(target=_exchange_worker, args=(r, 2, port, q, faces)) for r in range(2)]
     for p in procs:
         p.start()
@@ -175,7 +184,8 @@ def test_step_choreography_with_an_empty_rank_over_gloo():
     dt; the two other ranks receive each other's face slab."""
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_step_worker, args=(r, 3, 29615, q)) for r in range(3)]
+    port = _free_port()
+    procs = [ctx.Process(target=_step_worker, args=(r, 3, port, q)) for r in range(3)]
     for p in procs:
         p.start()
     res = sorted(q.get(timeout=120) for _ in procs)
