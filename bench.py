@@ -248,6 +248,88 @@ def live_mesh_leg(prob, args, stream):
     return out
 
 
+def cooling_workload() -> str:
+    """The cooling AMR workload of the metric's comparison: colliding winds
+    (table cooling + ionisation surrogate, 20,896 blocks) when the host can
+    hold the CPU port's arrays (~45 GB), else the radiative SNR at 64^3 root
+    cells (COOL_H + surrogate, 960 blocks).  WX3D_COOLING_WORKLOAD overrides."""
+    name = os.environ.get("WX3D_COOLING_WORKLOAD")
+    if name:
+        return name
+    try:
+        with open("/proc/meminfo") as f:
+            avail = next(int(l.split()[1]) * 1024 for l in f if l.startswith("MemAvailable:"))
+    except (OSError, StopIteration):
+        avail = 0
+    return "winds" if avail > 64 * 2**30 else "snr-h-c4"
+
+
+def cooling_leg(args, stream):
+    """The metric's three-way comparison on a cooling AMR workload, timed past
+    the 10-step dt ramp of main.f90 (whose dt lies below the surrogate's
+    training box): the batched form with the learned surrogate attached
+    (autotuned launch shape, replayed CUDA graph, MLP for trusted cells), the
+    same batched form without it, the plain GPU path (one synchronous
+    wx3d_step per step, launch shape from the mesh size, no graph, plain FP64
+    integrator), and the CPU port on a bounded sample.  Device times are CUDA
+    events on the library's stream; the CPU port is wall clock."""
+    import torch
+    from walicxe3d_b200.autotune import tune
+    from walicxe3d_b200.solver import from_problem
+    name = cooling_workload()
+    prob = build_problem(name)
+    ramp, K = 12, args.steps
+    out = {"workload": name, "description": WORKLOADS[name]["desc"], "blocks": prob.nblocks, "cells": prob.cells,
+           "unit": "Mcell-updates/s", "steps": K, "untimed_steps_first": ramp}
+
+    def timed(n, fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn(n)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        return {"value": prob.cells * n / (ms / 1e3) / 1e6, "ms_per_step": ms / n}
+
+    w = from_problem(prob)
+    w.set_stream(stream.cuda_stream)
+    tuned = tune(w, prob, cache=None, reps=1)
+    w.attach_surrogate()
+    w.run(ramp)
+    w.reset_status()
+    b = timed(K, w.run_async)
+    st = w.status()
+    sc, fc = int(st.surrogate_cells), int(st.fallback_cells)
+    b.update({"surrogate_cells": sc, "fallback_cells": fc, "share": sc / max(1, sc + fc),
+              "autotune": {"zsplit": tuned["zsplit"], "fused_viscous": tuned.get("fused")}})
+    out["batched_surrogate"] = b
+    w.detach_surrogate()
+    w.run(2)
+    out["batched"] = timed(K, w.run_async)
+    w.close()
+
+    wp = from_problem(prob)
+    wp.set_stream(stream.cuda_stream)
+    for _ in range(ramp):
+        wp.step()
+
+    def plain(n):
+        for _ in range(n):
+            wp.step()
+    out["plain"] = timed(K, plain)
+    wp.close()
+    out["surrogate_gain_vs_plain"] = out["batched_surrogate"]["value"] / out["plain"]["value"]
+    out["batched_gain_vs_plain"] = out["batched"]["value"] / out["plain"]["value"]
+    if not args.no_cpu_baseline:
+        v, n, secs = cpu_time_oracle(prob, 1000, float(os.environ.get("WX3D_CPU_BUDGET_S", "20")),
+                                     os.cpu_count() or 1)
+        out["cpu_port"] = {"value": v, "cores": os.cpu_count(), "kind": "port",
+                           "sample": f"{n} whole steps from the initial state in {secs:.1f}s, C++ FP64 "
+                                     f"restatement of the reference, OpenMP over blocks"}
+    return out
+
+
 def run_partition(args, prob, rank, world, dist):
     """One mesh shared by the ranks (walicxe3d_b200.partition): each owns a
     Hilbert share plus halo copies whose face slabs are exchanged over NCCL
@@ -316,6 +398,8 @@ def main():
     ap.add_argument("--zsplit", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-live-mesh", action="store_true", help="skip the live-mesh (admesh every step) leg")
+    ap.add_argument("--no-cooling", action="store_true",
+                    help="skip the cooling-workload leg (batched + surrogate vs batched vs plain GPU vs CPU port)")
     ap.add_argument("--partition", action="store_true",
                     help="strong scaling: the ranks share one mesh (halo exchange over NCCL) instead of replicas")
     ap.add_argument("--surrogate", action="store_true",
@@ -416,10 +500,16 @@ def main():
     if fig and "fp64_flops_per_cell" in fig and stage2_ms > 0:
         pk = fp64_peak_tflops(w.lib)
         ach = fig["fp64_flops_per_cell"] * prob.cells / (stage2_ms / 1e3) / 1e12
+        inst = fig.get("fp64_inst_per_cell")
         fp64 = {"achieved_tflops": ach, "peak_tflops": pk, "frac": (ach / pk) if pk else None,
                 "flops_per_cell": fig["fp64_flops_per_cell"],
+                "inst_per_cell": inst,
+                # FP64 instructions issued over the rate of DFMA chains (a DADD
+                # or DMUL takes the issue slot of a DFMA)
+                "inst_frac": (inst * prob.cells / (stage2_ms / 1e3) / (pk * 1e12 / 2)) if (pk and inst) else None,
                 "peak_source": "measured in this run (wx3d_measure_fp64_peak, DFMA chains)",
-                "note": "the stage kernels are bound by FP64 issue, not by HBM"}
+                "note": "per-cell figures from the ncu capture on Sedov 256^3; the stage kernels are "
+                        "latency-bound, below both their FP64 instruction bound and the HBM bound"}
 
     # --- the plain GPU path: the same kernels, one synchronous wx3d_step per
     # step (host round trip each step), default launch shape, no graph ---
@@ -477,6 +567,10 @@ def main():
     if rank == 0 and not args.no_live_mesh and not args.surrogate and prob.tree.maxlev > 1 and not prob.winds:
         live = live_mesh_leg(prob, args, stream)
 
+    cooling = None
+    if rank == 0 and world == 1 and not args.no_cooling:
+        cooling = cooling_leg(args, stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, n, secs = cpu_time_oracle(prob, 1000, float(os.environ.get("WX3D_CPU_BUDGET_S", "20")), os.cpu_count() or 1)
@@ -512,6 +606,7 @@ def main():
                             "returns time/dt/status to the host), download of the final state"},
             "gpu_launches": launches,
             "live_mesh": live,
+            "cooling": cooling,
             "plain_steps": plain,
             "surrogate": ({"attached": True, "surrogate_cells": sur_cells, "fallback_cells": fb_cells,
                            "share": sur_cells / max(1, sur_cells + fb_cells)} if args.surrogate else None),

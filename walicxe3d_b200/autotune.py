@@ -19,7 +19,13 @@ DEFAULT_CACHE = Path(os.environ.get("WX3D_TUNE_CACHE", Path.home() / ".cache" / 
 
 
 def signature(cfg, nblocks: int, levels) -> str:
-    lv = ",".join(str(int(l)) for l in sorted(set(levels)))
+    """Workload key: equation set, solver, limiter and the mesh's histogram
+    of blocks per level (the launch shape depends on how many blocks there
+    are and on the share of coarse/fine faces the levels bring)."""
+    hist = {}
+    for l in levels:
+        hist[int(l)] = hist.get(int(l), 0) + 1
+    lv = ",".join(f"{l}:{hist[l]}" for l in sorted(hist))
     return f"neq{cfg.neqtot}-s{cfg.solver_type}-l{cfg.limiter_type}-mhd{int(cfg.mhd)}-nb{nblocks}-lev{lv}"
 
 

@@ -315,6 +315,7 @@ void fill_phys(wx_ctx* c) {
   PhysParams& p = c->ph;
   p.gamma = f.gamma;
   p.cv = 1.0 / (f.gamma - 1.0);           // parameters.f90:373
+  p.inv_cv = 1.0 / p.cv;
   p.cfl = f.cfl;
   p.eta = f.visc_eta;
   p.mu0 = f.mu0; p.mui = f.mui; p.ion_thres = f.ion_thres;
@@ -1364,7 +1365,7 @@ int wx3d_update_prims(wx_ctx* c) {
   if (!ready(c)) return fail(c, WX_ERR_MESH, "no mesh");
   if (!c->dPrim) WX_CUDA(cudaMalloc(&c->dPrim, (size_t)c->max_blocks * c->neq * BCELLS * 8));
   c->k.prims<<<grid_for(c, (const void*)c->k.prims, 256, 0, c->nwork), 256, 0, c->stream>>>(c->dU, c->dPrim, c->dWork,
-                                                                                              c->nwork, c->dCtl, c->ph.cv);
+                                                                                              c->nwork, c->dCtl, c->ph.inv_cv);
   WX_LAUNCHED();
   return sync_check(c);
 }
@@ -2163,6 +2164,7 @@ int noalloc_table(const wx_config& cfg, int n, const int32_t* lb, DevBlock* hb, 
 void noalloc_phys(const wx_config& f, PhysParams& p) {
   p.gamma = f.gamma;
   p.cv = 1.0 / (f.gamma - 1.0);
+  p.inv_cv = 1.0 / p.cv;
   p.cfl = f.cfl;
   p.eta = f.visc_eta;
   p.mu0 = f.mu0; p.mui = f.mui; p.ion_thres = f.ion_thres;

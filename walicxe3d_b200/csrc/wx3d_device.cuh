@@ -51,6 +51,7 @@ struct __align__(16) DevCtl {
 
 struct PhysParams {
   double gamma, cv, cfl, eta;
+  double inv_cv;     // 1/cv: flow2prim multiplies by it instead of dividing by cv
   double mu0, mui, ion_thres;
   double d_sc, p_sc, e_sc, t_sc;
   double dtout;
@@ -115,20 +116,30 @@ __device__ __forceinline__ double sqrt_nr(double x) {
   return fma(0.5 * y, fma(-s, s, x), s);
 }
 
+// Brings the 128-byte line holding *p into L2 (no register result).
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // flow2prim (hydro_core.f90:323-378).  Returns istat: 0 ok, 1 pressure
-// floor, 2 density floor, -1 zero density.
+// floor, 2 density floor, -1 zero density.  The divisions by rho and by cv
+// of the reference are a Newton reciprocal of rho (IEEE division for zero,
+// subnormal, infinite or NaN densities, which rcp_nr does not take) and a
+// multiplication by inv_cv = 1/cv: the same values to within an ulp.
 template <int NEQ, bool MHD>
-__device__ __forceinline__ int flow2prim(const double* u, double* p, double cv, double* rinv_out = nullptr) {
+__device__ __forceinline__ int flow2prim(const double* u, double* p, double inv_cv, double* rinv_out = nullptr) {
   int istat = 0;
   if (u[0] == 0.0) istat = -1;
-  const double rinv = 1.0 / u[0];   // IEEE: u[0] may be zero or tiny here
+  double rinv;
+  if (fabs(u[0]) >= 2.2250738585072014e-308 && fabs(u[0]) <= 1.0e300) rinv = rcp_nr(u[0]);
+  else rinv = 1.0 / u[0];
   if (rinv_out) *rinv_out = rinv;
   p[0] = u[0];
   p[1] = u[1] * rinv;
   p[2] = u[2] * rinv;
   p[3] = u[3] * rinv;
-  double pr = (u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) * rinv) / cv;
-  if (MHD) pr = pr - 0.5 * (u[5] * u[5] + u[6] * u[6] + u[7] * u[7]) / cv;
+  double pr = (u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) * rinv) * inv_cv;
+  if (MHD) pr = pr - 0.5 * (u[5] * u[5] + u[6] * u[6] + u[7] * u[7]) * inv_cv;
   if (pr < 1.0e-30) { pr = 1.0e-30; if (istat == 0) istat = 1; }
   p[4] = pr;
   if (p[0] < 1.0e-40) {
@@ -255,7 +266,7 @@ __device__ __forceinline__ void riemann_hll_c(const double* pL, const double* pR
   xflux<NEQ, false>(pR, fR, cv);
   prim2flow<NEQ, false>(pL, uL, cv);
   prim2flow<NEQ, false>(pR, uR, cv);
-  const double inv = 1.0 / (sr - sl);
+  const double inv = rcp_nr(sr - sl);   // sl < 0 < sr here
   const double slsr = sl * sr;
 #pragma unroll
   for (int e = 0; e < NEQ; ++e) f[e] = (sr * fL[e] - sl * fR[e] + slsr * (uR[e] - uL[e])) * inv;
@@ -602,6 +613,40 @@ __device__ __forceinline__ double cell_dt(const double* p, const DevBlock& B, do
   const double cs = sqrt(g * p[4] / p[0]);
   return dmin(dmin(B.dx / (fabs(p[1]) + cs), B.dy / (fabs(p[2]) + cs)), B.dz / (fabs(p[3]) + cs));
 }
+
+// The CFL condition of a hydro cell as a signal speed over the cell size,
+// max_d (|u_d| + c)/dx_d, whose reciprocal is cell_dt's
+// min_d dx_d/(|u_d| + c).  A block's kernels keep the largest speed and take
+// one reciprocal at the end, so the per-cell work has no division.  idx..idz
+// are 1/dx..1/dz; rinv is 1/rho of flow2prim.
+__device__ __forceinline__ double cell_cfl_speed(const double* p, double rinv, double idx, double idy, double idz,
+                                                 double g) {
+  const double cs = sqrt_nr(g * p[4] * rinv);
+  return dmax(dmax((fabs(p[1]) + cs) * idx, (fabs(p[2]) + cs) * idy), (fabs(p[3]) + cs) * idz);
+}
+
+// One thread's running CFL reduction over the cells it visits: for hydro the
+// largest cell_cfl_speed (one reciprocal at the end), for MHD the smallest
+// cell_dt.  block() takes the inverse cell sizes of the block being walked.
+template <int NEQ, bool MHD>
+struct Cfl {
+  double acc = MHD ? 1.0e300 : 0.0;
+  double idx = 0.0, idy = 0.0, idz = 0.0;
+  __device__ __forceinline__ void block(const DevBlock& B) {
+    if (!MHD) { idx = 1.0 / B.dx; idy = 1.0 / B.dy; idz = 1.0 / B.dz; }
+  }
+  __device__ __forceinline__ void fold(const double* p, double rinv, const DevBlock& B, double g) {
+    fold(p, rinv, B, idx, idy, idz, g);
+  }
+  // the same with the inverse cell sizes passed in (block() not used)
+  __device__ __forceinline__ void fold(const double* p, double rinv, const DevBlock& B, double ix, double iy,
+                                       double iz, double g) {
+    if constexpr (MHD) acc = dmin(acc, cell_dt<NEQ, MHD>(p, B, g));
+    else acc = dmax(acc, cell_cfl_speed(p, rinv, ix, iy, iz, g));
+  }
+  // the thread's time step (infinite when it saw no cell)
+  __device__ __forceinline__ double dt() const { return MHD ? acc : 1.0 / acc; }
+};
 
 // Ordered bit patterns of positive doubles compare like the doubles.
 __device__ __forceinline__ void atomic_min_pos(unsigned long long* t, double v) {

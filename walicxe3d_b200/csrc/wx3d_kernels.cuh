@@ -55,11 +55,20 @@ __host__ __device__ constexpr int ring_channels() {
 
 constexpr int VPLANE = (NC + 2) * (NC + 2);  // a plane with its one-deep x/y frame
 
+// Per-block constants and status counters of a stage CTA, kept in shared
+// memory rather than in registers: dt/dx, dt/dy, dt/dz of the update, the
+// inverse cell sizes of the CFL fold, and the counts of pressure floors,
+// density floors, zero densities and non-finite results.
+struct StageConsts {
+  double dtdx, dtdy, dtdz, idx, idy, idz;
+  unsigned cnt[4];
+};
+
 template <int NEQ, bool MHD, int ORDER, bool VISC = false>
 __host__ __device__ constexpr size_t stage_smem_bytes() {
   return sizeof(double) * ((size_t)RING * ring_channels<NEQ, MHD, ORDER>() * Geo<ORDER>::PL + 2 * (size_t)NEQ * 17 * NC +
                            (VISC ? 2 * (size_t)NEQ * VPLANE : 0)) +
-         sizeof(DevBlock);
+         sizeof(DevBlock) + sizeof(StageConsts);
 }
 
 template <int ORDER>
@@ -150,16 +159,18 @@ __device__ __forceinline__ void iface_flux(const double* c0, const double* c1, c
 // non-finite values and folds the cell's CFL time step.
 template <int NEQ, bool MHD>
 __device__ __forceinline__ void visc_store(const StageParams& P, const DevBlock& B, const double* un, size_t o,
-                                           double& dtl, unsigned& nonfinite) {
+                                           Cfl<NEQ, MHD>& cfl, StageConsts& K) {
+  unsigned nonfinite = 0;
 #pragma unroll
   for (int e = 0; e < NEQ; ++e) {
     P.out[o + (size_t)e * BCELLS] = un[e];
     nonfinite += !isfinite(un[e]);
   }
+  if (nonfinite) atomicAdd(&K.cnt[3], nonfinite);
   if (P.do_dt) {
-    double p[NEQ];
-    flow2prim<NEQ, MHD>(un, p, P.ph.cv);
-    dtl = dmin(dtl, cell_dt<NEQ, MHD>(p, B, P.ph.gamma));
+    double p[NEQ], rinv;
+    flow2prim<NEQ, MHD>(un, p, P.ph.inv_cv, &rinv);
+    cfl.fold(p, rinv, B, K.idx, K.idy, K.idz, P.ph.gamma);
   }
 }
 
@@ -171,32 +182,28 @@ __device__ __forceinline__ void visc_store(const StageParams& P, const DevBlock&
 // counting the flow2prim floors of physical cells when `count`.
 template <int NEQ, bool MHD, int ORDER, int CH>
 __device__ __forceinline__ void store_cell(const PhysParams& ph, double* pl, int i, int j, const double* u, bool count,
-                                           unsigned& pf, unsigned& df, unsigned& zd) {
+                                           unsigned* cnt) {
   double p[NEQ], rinv;
-  const int st = flow2prim<NEQ, MHD>(u, p, ph.cv, &rinv);
+  const int st = flow2prim<NEQ, MHD>(u, p, ph.inv_cv, &rinv);
   if constexpr (CH > NEQ) {
     pl[NEQ * Geo<ORDER>::PL + hidx<ORDER>(i, j)] = sqrt_nr(ph.gamma * p[4] * rinv);
     pl[(NEQ + 1) * Geo<ORDER>::PL + hidx<ORDER>(i, j)] = rinv;
   }
-  if (count) {
-    pf += (st == 1);
-    df += (st == 2);
-    zd += (st < 0);
-  }
+  if (count && st != 0) atomicAdd(&cnt[st == 1 ? 0 : (st == 2 ? 1 : 2)], 1u);
 #pragma unroll
   for (int e = 0; e < NEQ; ++e) pl[e * Geo<ORDER>::PL + hidx<ORDER>(i, j)] = p[e];
 }
 
 template <int NEQ, bool MHD, int ORDER, int CH>
 __device__ __forceinline__ void load_plane(const StageParams& P, const DevBlock& B, int slot, int kk, int z0, int z1,
-                                           double* ring, unsigned& pf, unsigned& df, unsigned& zd) {
+                                           double* ring, unsigned* cnt, bool skip_interior = false) {
   const int t = threadIdx.x;
   const PhysParams& ph = P.ph;
   double* pl = ring + ring_slot(kk) * CH * Geo<ORDER>::PL;
   const bool inner = (kk >= 1 && kk <= NC);
   const bool frame = (kk >= z0 && kk <= z1);  // plane gets x/y fluxes
   const int nframe = frame ? (ORDER == 2 ? 128 : 64) : 0;
-  for (int c = t; c < PLANE + nframe; c += STAGE_THREADS) {
+  for (int c = skip_interior && t < PLANE ? t + STAGE_THREADS : t; c < PLANE + nframe; c += STAGE_THREADS) {
     int i, j;
     if (c < PLANE) { i = (c & 15) + 1; j = (c >> 4) + 1; }
     else {
@@ -212,7 +219,7 @@ __device__ __forceinline__ void load_plane(const StageParams& P, const DevBlock&
     double u[NEQ];
     if (inner && c < PLANE) load_cell<NEQ>(P.src, slot, i, j, kk, u);
     else gather_ghost<NEQ>(P.gsrc ? P.gsrc : P.src, B, slot, i, j, kk, u);
-    store_cell<NEQ, MHD, ORDER, CH>(ph, pl, i, j, u, c < PLANE && inner && frame, pf, df, zd);
+    store_cell<NEQ, MHD, ORDER, CH>(ph, pl, i, j, u, c < PLANE && inner && frame, cnt);
   }
 }
 
@@ -259,14 +266,13 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
   double* fys = fxs + NEQ * 17 * NC;                     // [NEQ][17][16 cols]
   double* wpl = fys + NEQ * 17 * NC;                     // VISC: [2][NEQ][VPLANE]
   DevBlock& B = *reinterpret_cast<DevBlock*>(wpl + (VISC ? 2 * NEQ * VPLANE : 0));
+  StageConsts& K = *reinterpret_cast<StageConsts*>(&B + 1);
   auto vq = [](int i, int j) { return i + (NC + 2) * j; };
-  double dtl = 1.0e300;
-  unsigned nonfinite = 0;
+  Cfl<NEQ, MHD> cfl;
   const int t = threadIdx.x;
   const int planes = NC / P.zsplit;
   const PhysParams& ph = P.ph;
-  const double dtp = P.ctl->dt * P.dt_factor;
-  unsigned pf = 0, df = 0, zd = 0;
+  if (t < 4) K.cnt[t] = 0;
 
   for (int w = blockIdx.x; w < P.nwork; w += gridDim.x) {
     const int slot = P.work[w / P.zsplit];
@@ -274,7 +280,15 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
     __syncthreads();
     if (t < (int)(sizeof(DevBlock) / 4)) reinterpret_cast<int*>(&B)[t] = reinterpret_cast<const int*>(P.blocks + slot)[t];
     __syncthreads();
-    const double dtdx = dtp / B.dx, dtdy = dtp / B.dy, dtdz = dtp / B.dz;
+    if (t == 0) {  // read after the prologue's barriers
+      const double dtp = P.ctl->dt * P.dt_factor;
+      K.dtdx = dtp / B.dx;
+      K.dtdy = dtp / B.dy;
+      K.dtdz = dtp / B.dz;
+      K.idx = 1.0 / B.dx;
+      K.idy = 1.0 / B.dy;
+      K.idz = 1.0 / B.dz;
+    }
     const int ci = (t & (NC - 1)) + 1, cj = (t >> 4) + 1;   // column of threads t < 256
     const int hc = hidx<ORDER>(ci, cj);
     double zprev[NEQ], znew[NEQ], zslope[NEQ];
@@ -285,7 +299,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
 
     // ---- prologue: planes z0-ORDER .. z0+ORDER-1, the z-interface z0-1/2,
     // then plane z0+ORDER into the slot of plane z0-ORDER ------------------
-    for (int kk = z0 - ORDER; kk <= z0 + ORDER - 1; ++kk) load_plane<NEQ, MHD, ORDER, CH>(P, B, slot, kk, z0, z1, ring, pf, df, zd);
+    for (int kk = z0 - ORDER; kk <= z0 + ORDER - 1; ++kk) load_plane<NEQ, MHD, ORDER, CH>(P, B, slot, kk, z0, z1, ring, K.cnt);
     __syncthreads();
     if (t < PLANE) {
       const int m = z0 - 1;
@@ -306,12 +320,32 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
       for (int e = 0; e < NEQ; ++e) wpl[((z0 - 1) & 1) * NEQ * VPLANE + e * VPLANE + vq(ci, cj)] = g[e];
     }
     __syncthreads();
-    load_plane<NEQ, MHD, ORDER, CH>(P, B, slot, z0 + ORDER, z0, z1, ring, pf, df, zd);
+    load_plane<NEQ, MHD, ORDER, CH>(P, B, slot, z0 + ORDER, z0, z1, ring, K.cnt);
     __syncthreads();
 
     for (int m = z0; m <= z1; ++m) {
       // ---- phase A: load plane m+ORDER+1; z-flux m+1/2; x/y fluxes of m ---
-      if (m + ORDER + 1 <= z1 + ORDER) load_plane<NEQ, MHD, ORDER, CH>(P, B, slot, m + ORDER + 1, z0, z1, ring, pf, df, zd);
+      {
+        // L2 prefetch, one plane period ahead, of the physical cells of the
+        // plane the next phase A loads and of the base plane the next phase B
+        // reads (16 lines of 128 bytes per equation and plane)
+        const int kq = t < 16 * NEQ ? m + ORDER + 2 : m + 1;
+        const double* arr = t < 16 * NEQ ? P.src : P.base;
+        const int r = t < 16 * NEQ ? t : t - 16 * NEQ;
+        if (r < 16 * NEQ && kq >= 1 && kq <= NC && kq <= z1 + ORDER && (t < 16 * NEQ || kq <= z1))
+          prefetch_l2(arr + cell_off(slot, NEQ, r >> 4, 1, 1, kq) + (size_t)(r & 15) * 16);
+      }
+      // the physical cell of each thread t < 256 is fetched here and
+      // converted into the ring after the fluxes, so its load latency
+      // overlaps them; the ghost frame is gathered and stored first
+      const int kl = m + ORDER + 1;
+      const bool late = t < PLANE && kl <= z1 + ORDER;
+      double ul[NEQ];
+      if (late) {
+        if (kl >= 1 && kl <= NC) load_cell<NEQ>(P.src, slot, ci, cj, kl, ul);
+        else gather_ghost<NEQ>(P.gsrc ? P.gsrc : P.src, B, slot, ci, cj, kl, ul);
+      }
+      if (kl <= z1 + ORDER) load_plane<NEQ, MHD, ORDER, CH>(P, B, slot, kl, z0, z1, ring, K.cnt, true);
       // one-deep x/y frame of W(m): UP ghosts of plane m, on threads 256..319,
       // which compute no z-flux and at most one x/y interface pair
       if (VISC && t >= PLANE && t < PLANE + 4 * NC) {
@@ -326,26 +360,22 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
           for (int e = 0; e < NEQ; ++e) wpl[(m & 1) * NEQ * VPLANE + e * VPLANE + vq(gi, gj)] = g[e];
         }
       }
-      if (t < PLANE) {
-        const double* c1 = ring + ring_slot(m) * CH * Geo<ORDER>::PL + hc;
-        const double* c2 = ring + ring_slot(m + 1) * CH * Geo<ORDER>::PL + hc;
-        const double* c3 = ring + ring_slot(m + 2) * CH * Geo<ORDER>::PL + hc;
-        iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 2, true>(nullptr, c1, c2, c3, ph, znew, zslope, false);
-      }
       if (t < 17 * NC) {
         const double* pp = ring + ring_slot(m) * CH * Geo<ORDER>::PL;
-        {  // x-interface between ii and ii+1 in row jx: a half-warp takes 16
-           // consecutive interfaces of one row (conflict-free shared loads),
-           // threads 256..271 the last interface of each row
-          const int ii = t < PLANE ? (t & 15) : NC, jx = t < PLANE ? (t >> 4) + 1 : t - PLANE + 1;
+        // x-interface between ii and ii+1 in row jx: a half-warp takes 16
+        // consecutive interfaces of one row (conflict-free shared loads),
+        // threads 256..271 the last interface of each row; y-interface
+        // between jj and jj+1 in column iy
+        const int ii = t < PLANE ? (t & 15) : NC, jx = t < PLANE ? (t >> 4) + 1 : t - PLANE + 1;
+        const int iy = (t & 15) + 1, jj = t >> 4;
+        {
           double f[NEQ];
           iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 0>(pp + hidx<ORDER>(ii - 1, jx), pp + hidx<ORDER>(ii, jx), pp + hidx<ORDER>(ii + 1, jx),
                                                  pp + hidx<ORDER>(ii + 2, jx), ph, f);
 #pragma unroll
           for (int e = 0; e < NEQ; ++e) fxs[(e * NC + (jx - 1)) * 17 + ii] = f[e];
         }
-        {  // y-interface between jj and jj+1 in column iy
-          const int iy = (t & 15) + 1, jj = t >> 4;
+        {
           double f[NEQ];
           iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 1>(pp + hidx<ORDER>(iy, jj - 1), pp + hidx<ORDER>(iy, jj), pp + hidx<ORDER>(iy, jj + 1),
                                                  pp + hidx<ORDER>(iy, jj + 2), ph, f);
@@ -353,6 +383,15 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
           for (int e = 0; e < NEQ; ++e) fys[(e * 17 + jj) * NC + (iy - 1)] = f[e];
         }
       }
+      if (t < PLANE) {  // z-flux m+1/2 last: znew is live only from here to phase B
+        const double* c1 = ring + ring_slot(m) * CH * Geo<ORDER>::PL + hc;
+        const double* c2 = ring + ring_slot(m + 1) * CH * Geo<ORDER>::PL + hc;
+        const double* c3 = ring + ring_slot(m + 2) * CH * Geo<ORDER>::PL + hc;
+        iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 2, true>(nullptr, c1, c2, c3, ph, znew, zslope, false);
+      }
+      if (late)
+        store_cell<NEQ, MHD, ORDER, CH>(ph, ring + ring_slot(kl) * CH * Geo<ORDER>::PL, ci, cj, ul,
+                                        kl >= 1 && kl <= NC && kl >= z0 && kl <= z1, K.cnt);
       __syncthreads();
       // ---- phase B: conservative update of plane m (godunov.f90:259-271) --
       if (t < PLANE) {
@@ -391,7 +430,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
           efield<ORDER>(pm + W, yr);
           efield<ORDER>(ring + ring_slot(m + 1) * CH * PL + hc, zu);
           efield<ORDER>(pm, ec);
-          const double hx = 0.5 * dtdx, hy = 0.5 * dtdy, hz = 0.5 * dtdz;
+          const double hx = 0.5 * K.dtdx, hy = 0.5 * K.dtdy, hz = 0.5 * K.dtdz;
           bcd[0] = __ldg(P.base + o + 5 * (size_t)BCELLS) - hy * (yr[2] - yl[2]) - hz * (-zu[1] + e_below[1]);
           bcd[1] = __ldg(P.base + o + 6 * (size_t)BCELLS) - hx * (-xr[2] + xl[2]) - hz * (zu[0] - e_below[0]);
           bcd[2] = __ldg(P.base + o + 7 * (size_t)BCELLS) - hx * (xr[1] - xl[1]) - hy * (-yr[0] + yl[0]);
@@ -399,13 +438,14 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
           for (int d = 0; d < 3; ++d) e_below[d] = ec[d];
         }
         double wv[NEQ];
+        const double dtdx = K.dtdx, dtdy = K.dtdy, dtdz = K.dtdz;
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) {
           const double fxl = fxs[(e * NC + (cj - 1)) * 17 + ci - 1], fxr = fxs[(e * NC + (cj - 1)) * 17 + ci];
           const double fyl = fys[(e * 17 + cj - 1) * NC + ci - 1], fyr = fys[(e * 17 + cj) * NC + ci - 1];
           double v = __ldg(P.base + o + (size_t)e * BCELLS) + dtdx * (fxl - fxr) + dtdy * (fyl - fyr) +
                      dtdz * (zprev[e] - znew[e]);
-          if (MHD && ph.eight_wave) v = v + dtp * s[e];
+          if (MHD && ph.eight_wave) v = v + P.ctl->dt * P.dt_factor * s[e];
           if (MHD && ph.flux_cd && e >= 5 && e <= 7) v = bcd[e - 5];
           if (VISC) wv[e] = v;
           else P.out[o + (size_t)e * BCELLS] = v;
@@ -422,7 +462,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
               un[e] = c + ph.eta * (+pe[vq(ci + 1, cj)] + pe[vq(ci - 1, cj)] + pe[vq(ci, cj + 1)] + pe[vq(ci, cj - 1)] +
                                     wv[e] + wb[e * VPLANE + vq(ci, cj)] - 6.0 * c);
             }
-            visc_store<NEQ, MHD>(P, B, un, o - NC * NC, dtl, nonfinite);
+            visc_store<NEQ, MHD>(P, B, un, o - NC * NC, cfl, K);
           }
 #pragma unroll
           for (int e = 0; e < NEQ; ++e) wb[e * VPLANE + vq(ci, cj)] = wv[e];
@@ -444,15 +484,12 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
         un[e] = c + ph.eta * (+pe[vq(ci + 1, cj)] + pe[vq(ci - 1, cj)] + pe[vq(ci, cj + 1)] + pe[vq(ci, cj - 1)] + g[e] +
                               wb[e * VPLANE + vq(ci, cj)] - 6.0 * c);
       }
-      visc_store<NEQ, MHD>(P, B, un, cell_off(slot, NEQ, 0, ci, cj, z1), dtl, nonfinite);
+      visc_store<NEQ, MHD>(P, B, un, cell_off(slot, NEQ, 0, ci, cj, z1), cfl, K);
     }
   }
-  flush_counts(P.ctl, pf, df, zd);
-  if (VISC) {
-    if (P.do_dt) block_min_dt(dtl, P.ctl);
-    nonfinite = __reduce_add_sync(0xffffffffu, nonfinite);
-    if ((t & 31) == 0 && nonfinite) atomicAdd(&P.ctl->cnt[3], (unsigned long long)nonfinite);
-  }
+  if (VISC && P.do_dt) block_min_dt(cfl.dt(), P.ctl);
+  __syncthreads();
+  if (t < 4 && K.cnt[t]) atomicAdd(&P.ctl->cnt[t], (unsigned long long)K.cnt[t]);
 }
 
 // ---------------------------------------------------------------------------
@@ -492,11 +529,11 @@ __global__ void __launch_bounds__(256) lax_kernel(LaxParams P) {
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         const double cc = d == 0 ? cx : (d == 1 ? cy : cz);
-        flow2prim<NEQ, MHD>(un[2 * d], pv, P.ph.cv);
+        flow2prim<NEQ, MHD>(un[2 * d], pv, P.ph.inv_cv);
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) tmp[e] = pv[d == 0 ? e : (d == 1 ? perm<1, MHD>(e) : perm<2, MHD>(e))];
         xflux<NEQ, MHD>(tmp, fr, P.ph.cv);
-        flow2prim<NEQ, MHD>(un[2 * d + 1], pv, P.ph.cv);
+        flow2prim<NEQ, MHD>(un[2 * d + 1], pv, P.ph.inv_cv);
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) tmp[e] = pv[d == 0 ? e : (d == 1 ? perm<1, MHD>(e) : perm<2, MHD>(e))];
         xflux<NEQ, MHD>(tmp, fl, P.ph.cv);
@@ -535,7 +572,7 @@ __global__ void __launch_bounds__(256) viscous_kernel(ViscParams P) {
   const int t = threadIdx.x;
   const int i = (t & 15) + 1, j = (t >> 4) + 1;
   const double eta = P.ph.eta;
-  double dtl = 1.0e300;
+  Cfl<NEQ, MHD> cfl;
   unsigned nonfinite = 0;
   auto q = [](int ii, int jj) { return ii + 18 * jj; };
   for (int w = blockIdx.x; w < P.nwork; w += gridDim.x) {
@@ -543,6 +580,7 @@ __global__ void __launch_bounds__(256) viscous_kernel(ViscParams P) {
     __syncthreads();
     if (t < (int)(sizeof(DevBlock) / 4)) reinterpret_cast<int*>(&B)[t] = reinterpret_cast<const int*>(P.blocks + slot)[t];
     __syncthreads();
+    cfl.block(B);
     double wm[NEQ], wc[NEQ], wp[NEQ];
     // W(k-1) for k=1 is the bottom ghost of UP
     if (P.zero_ghost) {
@@ -595,15 +633,15 @@ __global__ void __launch_bounds__(256) viscous_kernel(ViscParams P) {
         nonfinite += !isfinite(un[e]);
       }
       if (P.do_dt) {
-        double p[NEQ];
-        flow2prim<NEQ, MHD>(un, p, P.ph.cv);
-        dtl = dmin(dtl, cell_dt<NEQ, MHD>(p, B, P.ph.gamma));
+        double p[NEQ], rinv;
+        flow2prim<NEQ, MHD>(un, p, P.ph.inv_cv, &rinv);
+        cfl.fold(p, rinv, B, P.ph.gamma);
       }
 #pragma unroll
       for (int e = 0; e < NEQ; ++e) { wm[e] = wc[e]; wc[e] = wp[e]; }
     }
   }
-  if (P.do_dt) block_min_dt(dtl, P.ctl);
+  if (P.do_dt) block_min_dt(cfl.dt(), P.ctl);
   nonfinite = __reduce_add_sync(0xffffffffu, nonfinite);
   if ((t & 31) == 0 && nonfinite) atomicAdd(&P.ctl->cnt[3], (unsigned long long)nonfinite);
 }
@@ -621,18 +659,19 @@ struct DtParams {
 template <int NEQ, bool MHD>
 __global__ void __launch_bounds__(256) dt_kernel(DtParams P) {
   const int t = threadIdx.x;
-  double dtl = 1.0e300;
+  Cfl<NEQ, MHD> cfl;
   for (int w = blockIdx.x; w < P.nwork; w += gridDim.x) {
     const int slot = P.work[w];
     const DevBlock& B = P.blocks[slot];
+    cfl.block(B);
     for (int k = 1; k <= NC; ++k) {
-      double u[NEQ], p[NEQ];
+      double u[NEQ], p[NEQ], rinv;
       load_cell<NEQ>(P.u, slot, (t & 15) + 1, (t >> 4) + 1, k, u);
-      flow2prim<NEQ, MHD>(u, p, P.ph.cv);
-      dtl = dmin(dtl, cell_dt<NEQ, MHD>(p, B, P.ph.gamma));
+      flow2prim<NEQ, MHD>(u, p, P.ph.inv_cv, &rinv);
+      cfl.fold(p, rinv, B, P.ph.gamma);
     }
   }
-  block_min_dt(dtl, P.ctl);
+  block_min_dt(cfl.dt(), P.ctl);
 }
 
 __global__ void ctl_reset_dtmin_kernel(DevCtl* ctl) {

@@ -766,7 +766,7 @@ __device__ __forceinline__ void fallback_cell(const SurrParams& P, int id, doubl
   double u[NEQ], p[NEQ];
 #pragma unroll
   for (int e = 0; e < NEQ; ++e) u[e] = P.u[o + (size_t)e * BCELLS];
-  flow2prim<NEQ, false>(u, p, ph.cv);
+  flow2prim<NEQ, false>(u, p, ph.inv_cv);
   if (ph.cooling == WX_COOL_H) {
     h_cool_step<5>(u, p, dts, ph, &mloss);
   } else {
@@ -822,7 +822,7 @@ __global__ void __launch_bounds__(TILE, 4) surrogate_source_kernel(SurrParams P)
     double u[NEQ], p[NEQ];
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) u[e] = P.u[o + (size_t)e * BCELLS];
-    flow2prim<NEQ, false>(u, p, ph.cv);
+    flow2prim<NEQ, false>(u, p, ph.inv_cv);
     // gate: inside the training box and in a trusted bin (FP32 logs)
     const double dh = p[0] * inv_mu0;
     const double y0 = p[5] / dh;
@@ -971,6 +971,7 @@ PhysParams phys_from(const wx_config& f) {
   PhysParams p{};
   p.gamma = f.gamma;
   p.cv = 1.0 / (f.gamma - 1.0);
+  p.inv_cv = 1.0 / p.cv;
   p.cfl = f.cfl;
   p.eta = f.visc_eta;
   p.mu0 = f.mu0; p.mui = f.mui; p.ion_thres = f.ion_thres;

@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(256) source_kernel(SrcParams P) {
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) p[e] = P.prim[o + (size_t)e * BCELLS];
       } else {
-        flow2prim<NEQ, MHD>(u, p, ph.cv);
+        flow2prim<NEQ, MHD>(u, p, ph.inv_cv);
       }
       constexpr int fp = FP;
       if (HAS_PAS && do_hrate && do_cool && ph.eos == WX_EOS_H_RATE && ph.cooling == WX_COOL_H) {
@@ -151,11 +151,11 @@ __global__ void __launch_bounds__(256, 4) mark_kernel(MarkParams P) {
     auto commit = [&](int kk) {
       const int s = kk % 3;
       double p[NEQ];
-      flow2prim<NEQ, MHD>(ua, p, P.ph.cv);
+      flow2prim<NEQ, MHD>(ua, p, P.ph.inv_cv);
       pp[s][q(i, j)] = p[4];
       pr[s][q(i, j)] = p[0];
       if (kk >= 1 && kk <= NC && t < 64) {
-        flow2prim<NEQ, MHD>(ug, p, P.ph.cv);
+        flow2prim<NEQ, MHD>(ug, p, P.ph.inv_cv);
         pp[s][q(gi, gj)] = p[4];
         pr[s][q(gi, gj)] = p[0];
       }
@@ -288,7 +288,7 @@ __global__ void coarsen_batch_kernel(const double* __restrict__ from, double* __
 // Primitive variables of the physical cells (calcPrimsBlock CELLS_PHYS).
 template <int NEQ, bool MHD>
 __global__ void prims_kernel(const double* __restrict__ u, double* __restrict__ prim, const int32_t* __restrict__ work,
-                             int nwork, DevCtl* ctl, double cv) {
+                             int nwork, DevCtl* ctl, double inv_cv) {
   unsigned pf = 0, df = 0, zd = 0;
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const int slot = work[w];
@@ -297,7 +297,7 @@ __global__ void prims_kernel(const double* __restrict__ u, double* __restrict__ 
       double uu[NEQ], p[NEQ];
 #pragma unroll
       for (int e = 0; e < NEQ; ++e) uu[e] = u[o + (size_t)e * BCELLS];
-      const int st = flow2prim<NEQ, MHD>(uu, p, cv);
+      const int st = flow2prim<NEQ, MHD>(uu, p, inv_cv);
       pf += (st == 1); df += (st == 2); zd += (st < 0);
 #pragma unroll
       for (int e = 0; e < NEQ; ++e) prim[o + (size_t)e * BCELLS] = p[e];
