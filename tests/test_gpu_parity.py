@@ -601,7 +601,10 @@ def test_admesh_matches_oracle(ncpu):
     (amr.f90:44-133) on the device context and in the oracle.  The same
     blocks refine and coarsen into the same slots (first empty slot, as the
     reference's put), including slots freed earlier in the same call, and the
-    state after the last step matches."""
+    state after the last step matches.  Before each admesh the marking flags
+    are compared as well: from the second step on the device marking reads
+    the ghost primitives the step's first-order stage left behind instead of
+    gathering them."""
     prob = problems.amr_pulse()
     extra = 4 * prob.nblocks
     o = oracle.from_problem(prob, threads=ncpu, extra_slots=extra)
@@ -612,6 +615,9 @@ def test_admesh_matches_oracle(ncpu):
     for _ in range(12):
         o.step()
         g.step()
+        fo, fg = o.mark(), g.mark()
+        occ = g.local_blocks[:len(fg)] != -1
+        assert np.array_equal(fo[:len(fg)][occ], fg[occ])
         no, ng = o.admesh(), g.admesh()
         assert no == ng
         assert np.array_equal(o.blocks, g.local_blocks)

@@ -244,6 +244,12 @@ struct wx_ctx {
   int grid_stage = 0, grid_256 = 0;
   bool dt_valid = false;
   bool prestep = false;           // dW holds the state at the start of the last step
+  // ghost primitives for markByPhysical, left by the first-order stage once
+  // admesh is in use (GFRAME x (rho, p) per slot)
+  double* dG = nullptr;
+  bool mark_ghosts = false;       // the first-order stage writes dG
+  bool g_step = false;            // the step being enqueued writes dG
+  bool g_valid = false;           // dG holds the ghosts of the state in dW (with prestep)
   cudaGraphExec_t graph = nullptr;
   bool graph_valid = false;
   long long launches = 0;
@@ -449,7 +455,7 @@ int launch_wind(wx_ctx* c, double* u) {
 int launch_stage(wx_ctx* c, int order, const double* src, const double* base, double* out, double factor,
                  bool fused = false, const double* gsrc = nullptr) {
   StageParams P{src, base, out, c->dBlocks, c->dWork, c->nwork * c->zsplit, c->zsplit, c->dCtl, factor, c->ph,
-                sources_on(c) ? 0 : 1, gsrc ? gsrc : src};
+                sources_on(c) ? 0 : 1, gsrc ? gsrc : src, order == 1 && c->g_step ? c->dG : nullptr};
   auto fn = order == 1 ? c->k.stage1 : (fused ? c->k.stage2v : c->k.stage2);
   const size_t smem = order == 1 ? c->k.smem1 : (fused ? c->k.smem2v : c->k.smem2);
   const int grid = grid_for(c, (const void*)fn, STAGE_THREADS, smem, c->nwork * c->zsplit);
@@ -513,6 +519,8 @@ int solver_second(wx_ctx* c, bool finish_output) {
   WX_LAUNCHED();
   std::swap(c->dU, c->dW);
   c->prestep = true;
+  c->g_valid = c->g_step;
+  c->g_step = false;   // other first-order launches (the autotuner's) leave the record alone
   c->dt_valid = !sources_on(c);
   return WX_OK;
 }
@@ -520,6 +528,7 @@ int solver_second(wx_ctx* c, bool finish_output) {
 // Godunov(order)/LaxFriedrichs + doViscousStep; on return dU holds U^{n+1}.
 int enqueue_solver(wx_ctx* c, bool bump_it, bool finish_output) {
   const bool src = sources_on(c);
+  c->g_step = c->mark_ghosts && c->dG && c->hwind.empty() && c->cfg.solver_type != WX_SOLVER_LAX;
   step_begin_kernel<<<1, 1, 0, c->stream>>>(c->dCtl, c->ph.cfl, c->cfg.cooling_type != WX_COOL_NONE, c->ph.dtout,
                                             c->ph.t_sc, bump_it ? 1 : 0);
   WX_LAUNCHED();
@@ -542,6 +551,7 @@ int enqueue_solver(wx_ctx* c, bool bump_it, bool finish_output) {
     step_end_kernel<<<1, 1, 0, c->stream>>>(c->dCtl, finish_output ? 1 : 0);
     WX_LAUNCHED();
     c->prestep = true;
+    c->g_valid = false;
     c->dt_valid = !src;
     return WX_OK;
   }
@@ -761,6 +771,7 @@ int wx3d_finalize(wx_ctx* c) {
   cudaFree(c->dWind);
   cudaFree(c->dOps);
   cudaFree(c->dItems);
+  cudaFree(c->dG);
   if (c->hCtl) cudaFreeHost(c->hCtl);
   if (c->hblocks) cudaFreeHost(c->hblocks);
   if (c->hblocks_next) cudaFreeHost(c->hblocks_next);
@@ -908,6 +919,7 @@ static int commit_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nha
   while (c->zsplit < 8 && c->nwork * c->zsplit < 2 * c->nsm) c->zsplit *= 2;
   c->dt_valid = false;
   c->prestep = false;
+  c->g_valid = false;
   invalidate_graph(c);
   return WX_OK;
 }
@@ -1156,6 +1168,7 @@ int wx3d_upload_blocks(wx_ctx* c, int32_t nslots, const double* u) {
   WX_CUDA(cudaStreamSynchronize(c->stream));
   c->dt_valid = false;
   c->prestep = false;
+  c->g_valid = false;
   return WX_OK;
 }
 
@@ -1257,6 +1270,7 @@ int wx3d_read_bin(wx_ctx* c, const char* path, int32_t max_slots, int32_t* local
   if (nblocks) *nblocks = nloc;
   c->dt_valid = false;
   c->prestep = false;
+  c->g_valid = false;
   return WX_OK;
 }
 
@@ -1341,6 +1355,7 @@ int wx3d_upload_U_fortran(wx_ctx* c, int32_t nbmax, const double* U) {
   WX_CUDA(cudaStreamSynchronize(c->stream));
   c->dt_valid = false;
   c->prestep = false;
+  c->g_valid = false;
   return WX_OK;
 }
 
@@ -1618,7 +1633,7 @@ int wx3d_mark(wx_ctx* c, int32_t nslots, int32_t* flags) {
   if (!ready(c) || !flags || nslots > c->max_blocks) return WX_ERR_INVALID_ARG;
   WX_CUDA(cudaMemsetAsync(c->dFlags, 0xff, 4 * (size_t)c->max_blocks, c->stream));
   MarkParams P{c->dU, c->prestep ? c->dW : c->dU, c->dBlocks, c->dWork, c->nwork, c->dFlags, c->cfg.maxlev,
-               c->cfg.refine_thres, c->cfg.coarse_thres, c->ph};
+               c->cfg.refine_thres, c->cfg.coarse_thres, c->ph, c->prestep && c->g_valid ? c->dG : nullptr};
   c->k.mark<<<grid_for(c, (const void*)c->k.mark, 256, 0, c->nwork), 256, 0, c->stream>>>(P);
   WX_LAUNCHED();
   WX_CUDA(cudaMemcpyAsync(flags, c->dFlags, 4 * (size_t)nslots, cudaMemcpyDeviceToHost, c->stream));
@@ -1638,6 +1653,7 @@ int wx3d_refine(wx_ctx* c, int32_t father, const int32_t* ch) {
   WX_CUDA(cudaStreamSynchronize(c->stream));
   c->dt_valid = false;
   c->prestep = false;
+  c->g_valid = false;
   invalidate_graph(c);
   return WX_OK;
 }
@@ -1763,6 +1779,17 @@ int wx3d_admesh(wx_ctx* c, int32_t nbmax, int32_t* lb, int32_t* counts) {
   for (int s = 0; s < nbmax; ++s)
     if (lb[s] != c->local[s]) return fail(c, WX_ERR_MESH, "slot %d: local_blocks differs from the mesh last set", s);
   const Tree& T = c->tree;
+  // From now on the steps' first-order stage leaves the ghost primitives the
+  // marking reads (the record is allocated once; without it the marking
+  // gathers them from the neighbour slots).
+  if (!c->mark_ghosts) {
+    if (!c->dG && cudaMalloc(&c->dG, sizeof(double) * 2 * GFRAME * (size_t)c->max_blocks) != cudaSuccess) {
+      cudaGetLastError();
+      c->dG = nullptr;
+    }
+    c->mark_ghosts = c->dG != nullptr;
+    invalidate_graph(c);
+  }
   // markByPhysical on the device; empty slots keep FLAG_NONE
   std::vector<int32_t> mk(nbmax);
   int rc = wx3d_mark(c, nbmax, mk.data());
@@ -1871,6 +1898,7 @@ int wx3d_coarsen(wx_ctx* c, const int32_t* ch, int32_t father) {
   WX_CUDA(cudaStreamSynchronize(c->stream));
   c->dt_valid = false;
   c->prestep = false;
+  c->g_valid = false;
   invalidate_graph(c);
   return WX_OK;
 }

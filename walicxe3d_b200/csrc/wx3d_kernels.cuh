@@ -35,7 +35,24 @@ struct StageParams {
   int32_t do_dt;                    // fused viscous step: fold the CFL minimum of the result
   const double* __restrict__ gsrc;  // array the ghost cells are gathered from (src, or the
                                     // wind-imposed copy of U in the first stage of a wind run)
+  double* __restrict__ gframe;      // first-order stage: where to leave the ghost primitives
+                                    // markByPhysical reads (nullptr: not wanted)
 };
+
+// markByPhysical's ghost primitives (rho, p) of one block, left behind by the
+// first-order stage, which gathers and converts exactly these cells anyway:
+// entry (kk-1)*64 + h for entry h of the one-deep x/y frame of plane kk
+// (1..16), 1024 + c for cell c of the bottom ghost plane (kk = 0) and
+// 1280 + c for the top one (kk = 17).  Two doubles per entry.
+constexpr int GFRAME = 16 * 64 + 2 * PLANE;
+
+__device__ __forceinline__ int gframe_entry(int kk, int c) {
+  if (c >= PLANE) return (kk >= 1 && kk <= NC) ? (kk - 1) * 64 + (c - PLANE) : -1;
+  if (kk == 0) return 16 * 64 + c;
+  if (kk == NC + 1) return 16 * 64 + PLANE + c;
+  return -1;
+}
+
 
 // Ring plane geometry: 16x16 cells with the ORDER-deep x/y ghost frame.
 template <int ORDER>
@@ -74,6 +91,16 @@ __host__ __device__ constexpr size_t stage_smem_bytes() {
 template <int ORDER>
 __device__ __forceinline__ int hidx(int i, int j) { return (i + ORDER - 1) + Geo<ORDER>::W * (j + ORDER - 1); }
 __device__ __forceinline__ int ring_slot(int kk) { return (kk + 64) & (RING - 1); }
+
+// Copies the (rho, p) just stored in ring plane pl at (i, j) to entry e of
+// the block's ghost-primitive record.
+template <int ORDER>
+__device__ __forceinline__ void put_gframe(double* g, int slot, int e, const double* pl, int i, int j) {
+  double2 v;
+  v.x = pl[hidx<ORDER>(i, j)];
+  v.y = pl[4 * Geo<ORDER>::PL + hidx<ORDER>(i, j)];
+  reinterpret_cast<double2*>(g)[(size_t)slot * GFRAME + e] = v;
+}
 
 // Warp minimum of a positive time step folded into ctl->dtmin_bits.
 __device__ __forceinline__ void block_min_dt(double v, DevCtl* ctl) {
@@ -220,6 +247,10 @@ __device__ __forceinline__ void load_plane(const StageParams& P, const DevBlock&
     if (inner && c < PLANE) load_cell<NEQ>(P.src, slot, i, j, kk, u);
     else gather_ghost<NEQ>(P.gsrc ? P.gsrc : P.src, B, slot, i, j, kk, u);
     store_cell<NEQ, MHD, ORDER, CH>(ph, pl, i, j, u, c < PLANE && inner && frame, cnt);
+    if (ORDER == 1 && P.gframe) {
+      const int e = gframe_entry(kk, c);
+      if (e >= 0) put_gframe<ORDER>(P.gframe, slot, e, pl, i, j);
+    }
   }
 }
 
@@ -389,9 +420,11 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
         const double* c3 = ring + ring_slot(m + 2) * CH * Geo<ORDER>::PL + hc;
         iface_flux<NEQ, MHD, SOLVER, ORDER, LIM, 2, true>(nullptr, c1, c2, c3, ph, znew, zslope, false);
       }
-      if (late)
-        store_cell<NEQ, MHD, ORDER, CH>(ph, ring + ring_slot(kl) * CH * Geo<ORDER>::PL, ci, cj, ul,
-                                        kl >= 1 && kl <= NC && kl >= z0 && kl <= z1, K.cnt);
+      if (late) {
+        double* pl = ring + ring_slot(kl) * CH * Geo<ORDER>::PL;
+        store_cell<NEQ, MHD, ORDER, CH>(ph, pl, ci, cj, ul, kl >= 1 && kl <= NC && kl >= z0 && kl <= z1, K.cnt);
+        if (ORDER == 1 && P.gframe && kl == NC + 1) put_gframe<ORDER>(P.gframe, slot, gframe_entry(kl, t), pl, ci, cj);
+      }
       __syncthreads();
       // ---- phase B: conservative update of plane m (godunov.f90:259-271) --
       if (t < PLANE) {

@@ -118,6 +118,8 @@ struct MarkParams {
   int32_t maxlev;
   double refine_thres, coarse_thres;
   PhysParams ph;
+  const double* __restrict__ gframe;  // ghost (rho, p) left by the last step's first-order stage
+                                      // (GFRAME entries per block), or nullptr: gather from g
 };
 
 template <int NEQ, bool MHD>
@@ -143,21 +145,52 @@ __global__ void __launch_bounds__(256, 4) mark_kernel(MarkParams P) {
     const int side = t >> 4, r = (t & 15) + 1;
     const int gi = side == 0 ? 0 : (side == 1 ? NC + 1 : r);
     const int gj = side == 2 ? 0 : (side == 3 ? NC + 1 : r);
+    // with a ghost record (P.gframe) the ghost cells' (rho, p) are read from
+    // it, coalesced, instead of being gathered from the neighbour slots;
+    // they are the same values (the same gathers and flow2prim, done by the
+    // step's first-order stage)
+    const double2* G = P.gframe ? reinterpret_cast<const double2*>(P.gframe) + (size_t)slot * GFRAME : nullptr;
     double ua[NEQ], ug[NEQ];
     auto fetch = [&](int kk) {
-      get_cell<NEQ>((kk >= 1 && kk <= NC) ? P.u : P.g, B, slot, i, j, kk, ua);
-      if (kk >= 1 && kk <= NC && t < 64) gather_ghost<NEQ>(P.g, B, slot, gi, gj, kk, ug);
+      const bool inner = kk >= 1 && kk <= NC;
+      if (inner || !G) {
+        get_cell<NEQ>(inner ? P.u : P.g, B, slot, i, j, kk, ua);
+      } else {
+        const double2 v = G[kk == 0 ? 16 * 64 + t : 16 * 64 + PLANE + t];
+        ua[0] = v.x;
+        ua[1] = v.y;
+      }
+      if (inner && t < 64) {
+        if (!G) {
+          gather_ghost<NEQ>(P.g, B, slot, gi, gj, kk, ug);
+        } else {
+          const double2 v = G[(kk - 1) * 64 + t];
+          ug[0] = v.x;
+          ug[1] = v.y;
+        }
+      }
     };
     auto commit = [&](int kk) {
       const int s = kk % 3;
+      const bool inner = kk >= 1 && kk <= NC;
       double p[NEQ];
-      flow2prim<NEQ, MHD>(ua, p, P.ph.inv_cv);
-      pp[s][q(i, j)] = p[4];
-      pr[s][q(i, j)] = p[0];
-      if (kk >= 1 && kk <= NC && t < 64) {
-        flow2prim<NEQ, MHD>(ug, p, P.ph.inv_cv);
-        pp[s][q(gi, gj)] = p[4];
-        pr[s][q(gi, gj)] = p[0];
+      if (inner || !G) {
+        flow2prim<NEQ, MHD>(ua, p, P.ph.inv_cv);
+        pp[s][q(i, j)] = p[4];
+        pr[s][q(i, j)] = p[0];
+      } else {
+        pp[s][q(i, j)] = ua[1];
+        pr[s][q(i, j)] = ua[0];
+      }
+      if (inner && t < 64) {
+        if (!G) {
+          flow2prim<NEQ, MHD>(ug, p, P.ph.inv_cv);
+          pp[s][q(gi, gj)] = p[4];
+          pr[s][q(gi, gj)] = p[0];
+        } else {
+          pp[s][q(gi, gj)] = ug[1];
+          pr[s][q(gi, gj)] = ug[0];
+        }
       }
     };
     fetch(0);
