@@ -145,8 +145,8 @@ def cpu_time_oracle(prob, steps_max: int, budget_s: float, threads: int):
 def stage_figures(neq: int, fused: bool):
     """Per-cell DRAM bytes and FP64 flops of the corrector from the committed
     ncu summary (profiles/stage_kernels.json, measured on Sedov 256^3 at
-    neq 5); None for other equation counts, which that capture does not
-    cover."""
+    neq 5, with the DRAM bytes also measured on a four-level AMR mesh);
+    None for other equation counts, which those captures do not cover."""
     f = ROOT / "profiles" / "stage_kernels.json"
     if neq != 5 or not f.exists():
         return None
@@ -495,7 +495,10 @@ def main():
     step_bytes = 40 * neq * prob.cells       # 5 compulsory state passes per step
     step_achieved = step_bytes * args.steps * world / (ms / 1e3) / 1e9
     fig = stage_figures(neq, fused)
-    traffic = fig["dram_bytes_per_cell"] * prob.cells if fig else None
+    multilevel = len({int(prob.tree.level(int(b))) for b in prob.local_blocks}) > 1
+    per_cell = fig and (fig.get("dram_bytes_per_cell_amr") if multilevel and "dram_bytes_per_cell_amr" in fig
+                        else fig["dram_bytes_per_cell"])
+    traffic = per_cell * prob.cells if fig else None
     fp64 = None
     if fig and "fp64_flops_per_cell" in fig and stage2_ms > 0:
         pk = fp64_peak_tflops(w.lib)

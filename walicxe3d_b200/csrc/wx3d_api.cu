@@ -23,6 +23,7 @@
 #include "wx3d_kernels.cuh"
 #include "wx3d_source.cuh"
 
+
 using namespace wx;
 
 namespace {
@@ -460,6 +461,7 @@ int launch_stage(wx_ctx* c, int order, const double* src, const double* base, do
   const size_t smem = order == 1 ? c->k.smem1 : (fused ? c->k.smem2v : c->k.smem2);
   const int grid = grid_for(c, (const void*)fn, STAGE_THREADS, smem, c->nwork * c->zsplit);
   const int kind = (order == 2 || factor == 1.0) ? 1 : 0;
+  WX_CUDA(cudaMemsetAsync(&c->dCtl->work_next[order - 1], 0, sizeof(unsigned), c->stream));
   tick(c, kind, true);
   fn<<<grid, STAGE_THREADS, smem, c->stream>>>(P);
   WX_LAUNCHED();
@@ -568,7 +570,9 @@ int enqueue_sources(wx_ctx* c, int mode) {
   SrcParams P{c->dU, (mode & 4) ? c->dPrim : nullptr, c->dBlocks, c->dWork, c->nwork, mode, c->dCtl,
               c->dCool, c->dCool ? c->dCool + c->ncool : nullptr, c->ncool, c->ph, c->nZ};
   tick(c, 3, true);
-  c->k.src<<<grid_for(c, (const void*)c->k.src, 256, 0, c->nwork), 256, 0, c->stream>>>(P);
+  // one CTA per block: the hardware hands blocks to SMs as CTAs finish, and
+  // blocks of hot cells (the full Biro et al. loss) cost more than cold ones
+  c->k.src<<<std::max(1, c->nwork), 256, 0, c->stream>>>(P);
   WX_LAUNCHED();
   tick(c, 3, false);
   if (mode & 8) c->dt_valid = true;

@@ -47,6 +47,8 @@ struct __align__(16) DevCtl {
   unsigned long long cnt[4];      // pressure floor, density floor, zero density, non-finite
   unsigned long long maxloss_bits;
   unsigned long long sur[2];      // cells updated by the surrogate / by the plain integrator
+  unsigned work_next[2];          // next work item of the running first- and second-order stage
+  unsigned pad_[2];
 };
 
 struct PhysParams {

@@ -13,6 +13,7 @@
 
 namespace wx {
 
+
 // 17*16 x- and y-interfaces per plane on the first 272 threads; the plane
 // loads (320 cells at first order, 384 at second) spread over all 320, and
 // two CTAs per SM put five warps on every sub-partition
@@ -79,6 +80,8 @@ constexpr int VPLANE = (NC + 2) * (NC + 2);  // a plane with its one-deep x/y fr
 struct StageConsts {
   double dtdx, dtdy, dtdz, idx, idy, idz;
   unsigned cnt[4];
+  int next;   // the CTA's next work item
+  int pad_;
 };
 
 template <int NEQ, bool MHD, int ORDER, bool VISC = false>
@@ -305,7 +308,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
   const PhysParams& ph = P.ph;
   if (t < 4) K.cnt[t] = 0;
 
-  for (int w = blockIdx.x; w < P.nwork; w += gridDim.x) {
+  for (int w = blockIdx.x; w < P.nwork;) {
     const int slot = P.work[w / P.zsplit];
     const int z0 = 1 + (w % P.zsplit) * planes, z1 = z0 + planes - 1;
     __syncthreads();
@@ -519,6 +522,12 @@ __global__ void __launch_bounds__(STAGE_THREADS, (stage_ctas_per_sm<NEQ, MHD, OR
       }
       visc_store<NEQ, MHD>(P, B, un, cell_off(slot, NEQ, 0, ci, cj, z1), cfl, K);
     }
+    // items past the first wave go, in list order, to whichever CTA
+    // finishes first (the counter is zeroed before each launch): blocks at
+    // coarse/fine faces cost more, and a static stride left SMs idle
+    if (t == 0) K.next = (int)gridDim.x + (int)atomicAdd(&P.ctl->work_next[ORDER - 1], 1u);
+    __syncthreads();
+    w = K.next;
   }
   if (VISC && P.do_dt) block_min_dt(cfl.dt(), P.ctl);
   __syncthreads();
