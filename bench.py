@@ -593,7 +593,9 @@ def main():
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "path": "wx3d_run: CUDA graph of 2 steps replayed",
                        "autotune": tuned and {"zsplit": tuned["zsplit"], "fused_viscous": tuned.get("fused"),
-                                              "ms_per_pass": tuned["ms_per_pass"]}},
+                                              "ms_per_pass": tuned["ms_per_pass"], "key": tuned.get("key"),
+                                              "note": "one shape for all levels: every level's block is the same "
+                                                      "16^3 tile of one persistent launch"}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "kernel": "stage_kernel<ORDER=2> (corrector%s)" % (" + viscous step" if fused else ""),
