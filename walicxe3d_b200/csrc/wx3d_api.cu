@@ -125,17 +125,17 @@ struct Tree {
       acc += n;
     }
   }
-  int level(long long bID) const {  // meshlevel, amr.f90:637
+  __host__ __device__ int level(long long bID) const {  // meshlevel, amr.f90:637
     for (int l = 1; l <= maxlev; ++l) if (bID >= minID[l] && bID <= maxID[l]) return l;
     return -1;
   }
-  void coords(long long bID, int l, int x[3]) const {  // bcoords, amr.f90:972 (0-based here)
+  __host__ __device__ void coords(long long bID, int l, int x[3]) const {  // bcoords, amr.f90:972 (0-based here)
     long long loc = bID - minID[l];
     x[0] = (int)(loc % nb[l][0]);
     x[1] = (int)((loc / nb[l][0]) % nb[l][1]);
     x[2] = (int)(loc / ((long long)nb[l][0] * nb[l][1]));
   }
-  long long id(int l, const int x[3]) const {
+  __host__ __device__ long long id(int l, const int x[3]) const {
     return minID[l] + x[0] + (long long)nb[l][0] * (x[1] + (long long)nb[l][1] * x[2]);
   }
 };
@@ -220,6 +220,15 @@ struct wx_ctx {
   double* dStage = nullptr;  // staging slab for the Fortran layout
   size_t stage_bytes = 0;
   DevBlock* dBlocks = nullptr;
+  // neighbour-table build on the device (meshes without halo slots or wind
+  // sources): the new table goes to dBlocksNext and is swapped in on commit
+  DevBlock* dBlocksNext = nullptr;
+  int2* dHash = nullptr;          // bID -> slot, open addressing, hash_size entries
+  unsigned hash_size = 0;
+  int32_t* dLbBuf = nullptr;      // the slot list being built
+  int32_t* dMeshErr = nullptr;    // [3] first failing slots, then max_blocks face codes
+  bool next_on_device = false;    // the next table was built on the device
+  bool host_table_stale = false;  // hblocks lags dBlocks (built on the device)
   int32_t* dWork = nullptr;
   int32_t* dFlags = nullptr;
   int32_t* dOps = nullptr;   // admesh: refine/coarsen operations, 9 slots each
@@ -776,6 +785,10 @@ int wx3d_finalize(wx_ctx* c) {
   cudaFree(c->dOps);
   cudaFree(c->dItems);
   cudaFree(c->dG);
+  cudaFree(c->dBlocksNext);
+  cudaFree(c->dHash);
+  cudaFree(c->dLbBuf);
+  cudaFree(c->dMeshErr);
   if (c->hCtl) cudaFreeHost(c->hCtl);
   if (c->hblocks) cudaFreeHost(c->hblocks);
   if (c->hblocks_next) cudaFreeHost(c->hblocks_next);
@@ -905,16 +918,197 @@ static int build_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nhal
   return WX_OK;
 }
 
+// ---------------------------------------------------------------------------
+// The same neighbour table built on the device, for meshes without halo slots
+// or wind sources (the host build above stays for those): a bID -> slot hash
+// table filled by one thread per slot, then one thread per slot resolving its
+// six faces with the tree queries of amr.f90:439-1098, into dBlocksNext.  The
+// errors the host build reports are recorded as the smallest failing slot.
+
+__device__ __forceinline__ unsigned bid_hash(int id, unsigned mask) { return ((unsigned)id * 2654435761u) & mask; }
+
+__device__ __forceinline__ int hash_find(const int2* __restrict__ h, unsigned mask, long long id) {
+  if (id < 1 || id > 0x7fffffffLL) return -1;
+  unsigned k = bid_hash((int)id, mask);
+  for (unsigned probe = 0; probe <= mask; ++probe) {
+    const int2 e = h[k];
+    if (e.x == (int)id) return e.y;
+    if (e.x == -1) return -1;
+    k = (k + 1) & mask;
+  }
+  return -1;
+}
+
+// err[0]: first slot whose bID lies outside the tree; err[1]: a slot whose
+// bID another slot holds too
+__global__ void mesh_insert_kernel(const int32_t* __restrict__ lb, int n, Tree T, int2* h, unsigned mask, int* err) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int id = lb[s];
+  if (id == -1) return;
+  if (T.level(id) < 1) { atomicMin(&err[0], s); return; }
+  unsigned k = bid_hash(id, mask);
+  for (unsigned probe = 0; probe <= mask; ++probe) {
+    const int prev = atomicCAS(&h[k].x, -1, id);
+    if (prev == -1) { h[k].y = s; return; }
+    if (prev == id) { atomicMin(&err[1], s); return; }
+    k = (k + 1) & mask;
+  }
+  atomicMin(&err[1], s);
+}
+
+struct MeshGeom {
+  double xphystot, yphystot, zphystot, l_sc;
+  int nbroot[3];
+  int bc[6];
+};
+
+// err[2]: first slot with a face the tree queries cannot resolve; its code
+// (1 + 2 face: no active neighbour at the finest level, 2 + 2 face: not one
+// level apart) in code[slot]
+__global__ void mesh_table_kernel(const int32_t* __restrict__ lb, int n, int max_blocks, Tree T, MeshGeom G,
+                                  const int2* __restrict__ h, unsigned mask, DevBlock* out, int* err, int* code) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= max_blocks) return;
+  DevBlock b{};
+  const long long id = s < n ? lb[s] : -1;
+  const int l = id == -1 ? -1 : T.level(id);
+  if (l < 1) { out[s] = b; return; }   // empty slot, or outside the tree (reported by the insertion)
+  int x[3];
+  T.coords(id, l, x);
+  b.level = l;
+  b.bID = (int32_t)id;
+  for (int d = 0; d < 3; ++d) {
+    b.bc[d] = x[d] + 1;
+    b.sib[d] = l > 1 ? (x[d] & 1) : -1;
+  }
+  const double s2 = ldexp(1.0, l - 1);
+  b.dx = G.xphystot / ((double)(NC * G.nbroot[0]) * s2) / G.l_sc;
+  b.dy = G.yphystot / ((double)(NC * G.nbroot[1]) * s2) / G.l_sc;
+  b.dz = G.zphystot / ((double)(NC * G.nbroot[2]) * s2) / G.l_sc;
+  int bad = 0;
+  for (int f = 0; f < 6 && !bad; ++f) {
+    const int ax = f / 2, side = f & 1;
+    for (int q = 0; q < 4; ++q) b.fnb[f][q] = -1;
+    int y[3] = {x[0], x[1], x[2]};
+    y[ax] += side ? 1 : -1;
+    if (y[ax] < 0 || y[ax] >= T.nb[l][ax]) {
+      b.ftype[f] = WX_NEIGH_BOUNDARY;
+      b.fnb[f][0] = G.bc[f];
+      continue;
+    }
+    const int sn = hash_find(h, mask, T.id(l, y));
+    if (sn >= 0) { b.ftype[f] = WX_NEIGH_SAME; b.fnb[f][0] = sn; continue; }
+    if (l > 1) {
+      const int z[3] = {y[0] / 2, y[1] / 2, y[2] / 2};
+      const int sf = hash_find(h, mask, T.id(l - 1, z));
+      if (sf >= 0) { b.ftype[f] = WX_NEIGH_COARSER; b.fnb[f][0] = sf; continue; }
+    }
+    if (l >= T.maxlev) { bad = 1 + 2 * f; break; }
+    const int t1 = ax == 0 ? 1 : 0, t2 = ax == 2 ? 1 : 2;
+    b.ftype[f] = WX_NEIGH_FINER;
+    for (int q = 0; q < 4; ++q) {
+      int ch[3];
+      ch[ax] = 2 * y[ax] + (side ? 0 : 1);
+      ch[t1] = 2 * y[t1] + (q & 1);
+      ch[t2] = 2 * y[t2] + (q >> 1);
+      const int sc = hash_find(h, mask, T.id(l + 1, ch));
+      if (sc < 0) { bad = 2 + 2 * f; break; }
+      b.fnb[f][q] = sc;
+    }
+  }
+  if (bad) {
+    code[s] = bad;
+    atomicMin(&err[2], s);
+    out[s] = DevBlock{};
+    return;
+  }
+  out[s] = b;
+}
+
+// build_mesh on the device (no halo slots, no wind sources); on success the
+// new table is in dBlocksNext and next_on_device is set.
+static int build_mesh_gpu(wx_ctx* c, int32_t nslots, const int32_t* lb, std::vector<int32_t>& work) {
+  if (!c || !lb || nslots < 0) return WX_ERR_INVALID_ARG;
+  if (nslots > c->max_blocks) return fail(c, WX_ERR_INSUFICIENT_NBMAXPROC, "%d slots > max_blocks %d", nslots, c->max_blocks);
+  if (!c->dBlocksNext) {
+    unsigned hs = 16;
+    while (hs < 2u * (unsigned)c->max_blocks) hs <<= 1;
+    c->hash_size = hs;
+    if (cudaMalloc(&c->dBlocksNext, sizeof(DevBlock) * (size_t)c->max_blocks) != cudaSuccess ||
+        cudaMalloc(&c->dHash, sizeof(int2) * (size_t)hs) != cudaSuccess ||
+        cudaMalloc(&c->dLbBuf, 4 * (size_t)c->max_blocks) != cudaSuccess ||
+        cudaMalloc(&c->dMeshErr, 4 * (3 + (size_t)c->max_blocks)) != cudaSuccess)
+      return fail(c, WX_ERR_CUDA, "device neighbour-table buffers");
+  }
+  work.clear();
+  work.reserve(nslots);
+  for (int s = 0; s < nslots; ++s)
+    if (lb[s] != -1) work.push_back(s);
+  const int big = 0x7fffffff;
+  const int init[3] = {big, big, big};
+  if (nslots > 0) WX_CUDA(cudaMemcpyAsync(c->dLbBuf, lb, 4 * (size_t)nslots, cudaMemcpyHostToDevice, c->stream));
+  WX_CUDA(cudaMemcpyAsync(c->dMeshErr, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+  WX_CUDA(cudaMemsetAsync(c->dHash, 0xff, sizeof(int2) * (size_t)c->hash_size, c->stream));
+  const unsigned mask = c->hash_size - 1;
+  if (nslots > 0) {
+    mesh_insert_kernel<<<(nslots + 255) / 256, 256, 0, c->stream>>>(c->dLbBuf, nslots, c->tree, c->dHash, mask, c->dMeshErr);
+    WX_LAUNCHED();
+  }
+  MeshGeom G;
+  G.xphystot = c->cfg.xphystot; G.yphystot = c->cfg.yphystot; G.zphystot = c->cfg.zphystot; G.l_sc = c->cfg.l_sc;
+  G.nbroot[0] = c->cfg.nbrootx; G.nbroot[1] = c->cfg.nbrooty; G.nbroot[2] = c->cfg.nbrootz;
+  for (int f = 0; f < 6; ++f) G.bc[f] = c->cfg.bc[f];
+  mesh_table_kernel<<<(c->max_blocks + 255) / 256, 256, 0, c->stream>>>(c->dLbBuf, nslots, c->max_blocks, c->tree, G,
+                                                                        c->dHash, mask, c->dBlocksNext, c->dMeshErr,
+                                                                        c->dMeshErr + 3);
+  WX_LAUNCHED();
+  int herr[3];
+  WX_CUDA(cudaMemcpyAsync(herr, c->dMeshErr, sizeof(herr), cudaMemcpyDeviceToHost, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  if (herr[0] != big || herr[1] != big) {
+    if (herr[0] < herr[1]) return fail(c, WX_ERR_MESH, "slot %d: bID %d outside the tree", herr[0], lb[herr[0]]);
+    return fail(c, WX_ERR_MESH, "bID %d registered twice", lb[herr[1]]);
+  }
+  if (herr[2] != big) {
+    int code = 0;
+    WX_CUDA(cudaMemcpy(&code, c->dMeshErr + 3 + herr[2], 4, cudaMemcpyDeviceToHost));
+    const int f = (code - 1) / 2;
+    if ((code - 1) % 2 == 0) return fail(c, WX_ERR_MESH, "bID %d face %d: no active neighbour", lb[herr[2]], f + 1);
+    return fail(c, WX_ERR_MESH, "bID %d face %d: neighbour region is neither same, coarser nor finer by one", lb[herr[2]], f + 1);
+  }
+  c->next_on_device = true;
+  return WX_OK;
+}
+
+// The host copy of the table, for the host readers (neighbour queries, the
+// wind-sphere flags), after a build on the device.
+static int sync_host_table(wx_ctx* c) {
+  if (!c->host_table_stale) return WX_OK;
+  WX_CUDA(cudaMemcpyAsync(c->hblocks, c->dBlocks, sizeof(DevBlock) * (size_t)c->max_blocks, cudaMemcpyDeviceToHost,
+                          c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  c->host_table_stale = false;
+  return WX_OK;
+}
+
 // Makes the mesh that build_mesh left in hblocks_next the context's.
 static int commit_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nhalo, std::vector<int32_t>& work) {
   c->local.assign(c->max_blocks, -1);
   std::copy(lb, lb + nslots, c->local.begin());
   c->nhalo = nhalo;
-  std::swap(c->hblocks, c->hblocks_next);
   c->work = std::move(work);
   c->nwork = (int)c->work.size();
   c->mesh_set = true;
-  WX_CUDA(cudaMemcpyAsync(c->dBlocks, c->hblocks, sizeof(DevBlock) * c->max_blocks, cudaMemcpyHostToDevice, c->stream));
+  if (c->next_on_device) {
+    std::swap(c->dBlocks, c->dBlocksNext);
+    c->next_on_device = false;
+    c->host_table_stale = true;
+  } else {
+    std::swap(c->hblocks, c->hblocks_next);
+    WX_CUDA(cudaMemcpyAsync(c->dBlocks, c->hblocks, sizeof(DevBlock) * c->max_blocks, cudaMemcpyHostToDevice, c->stream));
+    c->host_table_stale = false;
+  }
   if (!c->work.empty())
     WX_CUDA(cudaMemcpyAsync(c->dWork, c->work.data(), 4 * c->work.size(), cudaMemcpyHostToDevice, c->stream));
   WX_CUDA(cudaStreamSynchronize(c->stream));
@@ -928,9 +1122,17 @@ static int commit_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nha
   return WX_OK;
 }
 
+// The device build serves meshes without halo slots or wind sources.
+static int build_any(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nhalo, const int32_t* halo,
+                     std::vector<int32_t>& work) {
+  if (c && nhalo == 0 && c->hwind.empty()) return build_mesh_gpu(c, nslots, lb, work);
+  if (c) c->next_on_device = false;
+  return build_mesh(c, nslots, lb, nhalo, halo, work);
+}
+
 int wx3d_set_mesh_halo(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nhalo, const int32_t* halo) {
   std::vector<int32_t> work;
-  const int rc = build_mesh(c, nslots, lb, nhalo, halo, work);
+  const int rc = build_any(c, nslots, lb, nhalo, halo, work);
   return rc ? rc : commit_mesh(c, nslots, lb, nhalo, work);
 }
 
@@ -960,6 +1162,8 @@ int wx3d_set_winds(wx_ctx* c, int32_t nwind, const wx_wind* winds) {
       return fail(c, WX_ERR_INVALID_ARG, "wind %d: radius, vinf, mdot and mu must be positive", w);
     std::copy(v, v + 12, h.begin() + 12 * w);
   }
+  const int rs = sync_host_table(c);
+  if (rs) return rs;
   std::vector<double> prev = c->hwind;
   c->hwind = h;
   int bad = -1;
@@ -1157,6 +1361,8 @@ int wx3d_autotune(wx_ctx* c, int32_t reps, double* ms5, int32_t* best) {
 
 int wx3d_get_neighbours(wx_ctx* c, int32_t nslots, int32_t* ft, int32_t* fs) {
   if (!c || !ft || !fs || nslots > c->max_blocks) return WX_ERR_INVALID_ARG;
+  const int rc = sync_host_table(c);
+  if (rc) return rc;
   for (int s = 0; s < nslots; ++s)
     for (int f = 0; f < 6; ++f) {
       ft[s * 6 + f] = c->hblocks[s].ftype[f];
@@ -1856,7 +2062,7 @@ int wx3d_admesh(wx_ctx* c, int32_t nbmax, int32_t* lb, int32_t* counts) {
   // the new mesh is checked before any data moves, so a refused mesh
   // leaves the state and the slot registry as they were
   std::vector<int32_t> work;
-  if ((rc = build_mesh(c, nbmax, L.lb.data(), 0, nullptr, work))) return rc;
+  if ((rc = build_any(c, nbmax, L.lb.data(), 0, nullptr, work))) return rc;
   // data: refinements, then coarsenings.  Each pass first copies the blocks
   // it reads (fathers, or siblings) from U into UP at the same slots -- UP
   // holds nothing between steps, the next predictor overwrites it -- then
