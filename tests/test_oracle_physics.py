@@ -190,3 +190,59 @@ def test_a_process_without_blocks_takes_the_output_clamped_dt():
     s = o.state
     assert (s.time, s.dt, s.it, s.nextout) == (want, want, 4, 2)
     o.close()
+
+
+def test_hrate_closed_form_solves_the_rate_equation(ncpu):
+    """updateNeutralFraction (hrate.f90:82-142) writes, for each cell at fixed
+    T, the closed-form solution over dt of the rate equation of the neutral
+    fraction y = n_HI / n_H,
+        dy/dt = n_H [alpha (1 - y)(1 - y + xi) - col y (1 - y + xi)]
+              = n_H (a y^2 + b y + c),
+    recombination alpha(T) = 2.55e-13 (1e4/T)^0.79 and collisional
+    ionisation col(T) = 5.83e-11 sqrt(T) exp(-157828/T) (hrate.f90:51-75),
+    electrons n_e = n_H (1 - y + xi), xi = 1e-4 from metals, with the density
+    and temperature hrate.f90 itself forms (dh = PRIM(1)/mu0 and calcTemp's
+    EOS_H_RATE expression, hydro_core.f90:231-270).  A physics pin
+    independent of the restatement: the oracle's result against a numerical
+    integration of that equation (scipy solve_ivp, DOP853, rtol 1e-11) for
+    cells across n_H, T and y0, at two step lengths."""
+    from scipy.integrate import solve_ivp
+
+    mu0 = 1.3
+    cfg = C.Config(npassive=1, eos_type=C.EOS_H_RATE, cooling_type=C.COOL_NONE, nbroot=(1, 1, 1), maxlev=1,
+                   gamma=5.0 / 3.0, l_sc=C.PC, d_sc=mu0 * C.AMU, v_sc=1.0e5, box=(C.PC,) * 3)
+    rng = np.random.default_rng(20261203)
+    n = 16 ** 3
+    nH = 10.0 ** rng.uniform(-2, 3, n)                  # cm^-3
+    T = 10.0 ** rng.uniform(3.5, 6.0, n)                # K
+    y0 = rng.uniform(0.01, 0.99, n)
+    rho = nH * mu0 * C.AMU                              # g cm^-3
+    p_phys = (2.0 - y0) * nH * C.KB * T                 # P = (n_H + n_e) k T, n_e = n_H (1 - y)
+    prim = np.zeros((1, cfg.neqtot, 16, 16, 16))
+    prim[0, 0] = (rho / cfg.d_sc).reshape(16, 16, 16)
+    prim[0, 4] = (p_phys / cfg.p_sc).reshape(16, 16, 16)
+    prim[0, 5] = (y0 * rho / cfg.d_sc / mu0).reshape(16, 16, 16)    # n_HI = y n_H, n_H = rho / mu0
+    U = problems.prim2flow(cfg, prim)
+    t_sc = cfg.l_sc / cfg.v_sc
+    pick = rng.choice(n, 40, replace=False)
+    xi = 1.0e-4
+    for dt_yr in (1.0, 300.0):
+        o = oracle.Oracle(cfg, 1, threads=ncpu)
+        o.set_blocks([1])
+        o.set_U(U)
+        o.set_state(0.0, dt_yr * C.YR / t_sc, 0, 1, 0)
+        o.update_prims()
+        o.update_neutral_fraction()
+        P = o.PRIM[0]
+        y1 = (P[5] / (P[0] / mu0)).ravel()
+        o.close()
+        rho_c, p_c = P[0].ravel(), P[4].ravel()
+        for c in pick:
+            dh = rho_c[c] / mu0
+            Tc = p_c[c] / (2.0 * dh - y0[c] * dh) * cfg.p_sc / C.KB
+            a_rec = 2.55e-13 * (1.0e4 / Tc) ** 0.79
+            col = 5.83e-11 * np.sqrt(Tc) * np.exp(-157828.0 / Tc)
+            f = lambda t, y: [dh * (a_rec * (1 - y[0]) * (1 - y[0] + xi) - col * y[0] * (1 - y[0] + xi))]
+            sol = solve_ivp(f, (0.0, dt_yr * C.YR), [y0[c]], method="DOP853", rtol=1e-11, atol=1e-14)
+            assert sol.success
+            assert abs(y1[c] - sol.y[0, -1]) < 1e-7, (c, dh, Tc, y0[c], dt_yr, y1[c], sol.y[0, -1])
