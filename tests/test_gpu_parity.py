@@ -336,6 +336,64 @@ def test_sedov_256_conservation_and_symmetry():
     assert np.abs(G - G.transpose(2, 1, 0)).max() <= 1e-12 * scale
 
 
+SEDOV_XI0_GAMMA_5_3 = 1.15167   # E = alpha rho R^5 / t^2, alpha(5/3) = 0.4936 (Kamm & Timmes 2007)
+
+
+def _sedov_radial_density(prob, U):
+    """Mean density in radial shells of one cell width about the box centre:
+    (shell centres, mean density)."""
+    from walicxe3d_b200.mesh import cell_centres
+
+    n = prob.cfg.nbroot[0] * 16
+    xyz = cell_centres(prob.cfg, prob.tree, [int(b) for b in prob.local_blocks])
+    r = np.sqrt(((xyz - 0.5) ** 2).sum(axis=1)).ravel()
+    rho = U[:, 0].ravel()
+    nbins = n // 2
+    idx = np.minimum((r * n).astype(np.int64), nbins)
+    ok = idx < nbins
+    mean = np.bincount(idx[ok], weights=rho[ok], minlength=nbins) / np.maximum(
+        np.bincount(idx[ok], minlength=nbins), 1)
+    return (np.arange(nbins) + 0.5) / n, mean
+
+
+def test_sedov_taylor_blast_radius_converges():
+    """Physics check of the GPU path on a strong point blast: the shock radius
+    approaches the Sedov-Taylor similarity solution R = xi0 (E t^2/rho)^(1/5)
+    (gamma = 5/3, xi0 = 1.15167) as the mesh is refined (64^3, 128^3, 256^3
+    cells), and the shell-averaged peak density rises towards the
+    strong-shock limit (gamma+1)/(gamma-1) = 4 without passing it.  The run
+    stops at the output time where R = 0.3 (the clip to dtout lands on it
+    exactly); the shock is located where the shell-averaged density falls
+    through the middle of ambient and peak, outside the peak."""
+    r_target = 0.3
+    t_target = (r_target / SEDOV_XI0_GAMMA_5_3) ** 2.5     # rho = E = 1
+    errs, peaks = [], []
+    for nroot in (4, 8, 16):
+        prob = problems.sedov(nroot, radius_cells=3.0)
+        prob.cfg.visc_eta = 0.0
+        prob.cfg.dtout = t_target
+        g = from_problem(prob)
+        try:
+            for _ in range(5000):
+                s = g.step()
+                if s.dumpout:
+                    break
+            assert s.dumpout and s.time == pytest.approx(t_target, rel=1e-14)
+            U = g.download()
+        finally:
+            g.close()
+        rc, prof = _sedov_radial_density(prob, U)
+        ip = int(np.argmax(prof))
+        half = 0.5 * (1.0 + prof[ip])
+        j = ip + int(np.argmax(prof[ip:] < half))              # first shell outside the peak below half
+        r_shock = rc[j - 1] + (half - prof[j - 1]) / (prof[j] - prof[j - 1]) * (rc[j] - rc[j - 1])
+        errs.append(abs(r_shock / r_target - 1.0))
+        peaks.append(prof[ip])
+    assert errs[0] > errs[1] > errs[2], errs
+    assert errs[2] < 0.02, errs
+    assert peaks[0] < peaks[1] < peaks[2] < 4.0, peaks
+
+
 def test_blast_amr_full_size_matches_oracle(ncpu):
     """The benchmark's headline mesh at full size (8^3 roots, 5 levels,
     11,600 blocks, 47.5M cells), stepped through the replayed CUDA graph of
