@@ -1,5 +1,6 @@
 """Physics pins of the CPU oracle (the reference ships no golden data):
-exact Riemann solutions, FP64 conservation, symmetry, Brio-Wu structure."""
+exact Riemann solutions, FP64 conservation, symmetry, Brio-Wu structure,
+the hrate rate equation and the table-cooling loss law."""
 import numpy as np
 import pytest
 
@@ -246,3 +247,63 @@ def test_hrate_closed_form_solves_the_rate_equation(ncpu):
             sol = solve_ivp(f, (0.0, dt_yr * C.YR), [y0[c]], method="DOP853", rtol=1e-11, atol=1e-14)
             assert sol.success
             assert abs(y1[c] - sol.y[0, -1]) < 1e-7, (c, dh, Tc, y0[c], dt_yr, y1[c], sol.y[0, -1])
+
+
+def test_table_cooling_removes_n2_lambda_of_the_thermal_energy(ncpu):
+    """apply_cooling (cooling.f90:285-371) integrates dE_th/dt = -n^2
+    Lambda(T) over one step with the coefficient frozen at the start,
+    E_th(dt) = E_th exp(-n^2 Lambda dt / E_th), n = rho / (mui m_u), with
+    Lambda interpolated log-linearly in the table (find_coef,
+    cooling.f90:378-419), extrapolated as T^(1/2) above its last row and zero
+    below its first, and the loss clipped at cooling_limit.  A pin of the
+    restatement's units (d_sc, p_sc, t_sc, e_sc), temperature (calcTemp's
+    EOS_SINGLE_SPECIE: p = n k T, n = rho / (mu0 m_u)) and table lookup: the
+    oracle's pressure ratio against that expression evaluated here in
+    physical cgs units with numpy's interpolation, for cells across n and T
+    inside, above and below the table."""
+    mu0 = 1.3
+    cfg = C.Config(npassive=0, eos_type=C.EOS_SINGLE_SPECIE, cooling_type=C.COOL_TABLE, nbroot=(1, 1, 1), maxlev=1,
+                   gamma=5.0 / 3.0, l_sc=C.PC, d_sc=mu0 * C.AMU, v_sc=1.0e5, box=(C.PC,) * 3)
+    logT_tab, b_tab = problems.cooling_table_synthetic(200)
+    logL_tab = -b_tab
+    rng = np.random.default_rng(20261204)
+    n = 16 ** 3
+    ncm = 10.0 ** rng.uniform(-1, 2, n)                       # cm^-3, n = rho / (mu0 m_u)
+    logT = rng.uniform(4.0, 9.0, n)
+    logT[:200] = rng.uniform(3.5, 3.99, 200)                  # below the table: no cooling
+    logT[200:400] = rng.uniform(9.0, 9.5, 200)                # above it: T^(1/2) extrapolation
+    T = 10.0 ** logT
+    rho = ncm * mu0 * C.AMU
+    p_phys = ncm * C.KB * T
+    prim = np.zeros((1, cfg.neqtot, 16, 16, 16))
+    prim[0, 0] = (rho / cfg.d_sc).reshape(16, 16, 16)
+    prim[0, 4] = (p_phys / cfg.p_sc).reshape(16, 16, 16)
+    U = problems.prim2flow(cfg, prim)
+
+    lam = np.where(logT >= logT_tab[-1], 10.0 ** (logL_tab[-1] + 0.5 * (logT - logT_tab[-1])),
+                   10.0 ** np.interp(logT, logT_tab, logL_tab))
+    lam[logT < logT_tab[0]] = 0.0
+    n_cool = rho / (cfg.mui * C.AMU)
+    e_th = p_phys / (cfg.gamma - 1.0)
+    t_sc = cfg.l_sc / cfg.v_sc
+    for dt_yr in (1.0e2, 1.0e4):                               # the longer step clips the densest cells
+        x = n_cool ** 2 * lam * (dt_yr * C.YR) / e_th
+        want = np.maximum(np.exp(-x), 1.0 - cfg.cooling_limit)
+        o = oracle.Oracle(cfg, 1, threads=ncpu)
+        o.set_blocks([1])
+        o.set_U(U)
+        o.set_cooltable(logT_tab, b_tab)
+        o.set_state(0.0, dt_yr * C.YR / t_sc, 0, 1, 0)
+        o.update_prims()
+        p0 = o.PRIM[0][4].ravel().copy()
+        maxloss = o.cooling()
+        p1 = o.PRIM[0][4].ravel().copy()
+        eng = o.U[0][4].ravel()
+        o.close()
+        got = p1 / p0
+        assert np.all(got[:200] == 1.0)
+        assert np.abs(got / want - 1.0).max() < 1e-12
+        assert np.allclose(eng, p1 / (cfg.gamma - 1.0), rtol=1e-14, atol=0)
+        assert maxloss == pytest.approx((1.0 - np.exp(-x)).max(), rel=1e-12)
+        if dt_yr > 1e3:
+            assert np.any(np.exp(-x) < 1.0 - cfg.cooling_limit)
