@@ -217,7 +217,9 @@ int wx3d_set_fusion(wx_ctx* ctx, int32_t fuse_viscous);
  * predictor, the corrector and the viscous step (reps passes each) -- on
  * the live state, without changing it -- for five shapes: whole blocks with
  * the viscous step fused into the corrector, whole blocks with a separate
- * viscous kernel, and 2, 4, 8 z-slabs per block; keeps the fastest.
+ * viscous kernel, and 2, 4, 8 z-slabs per block; keeps the fastest.  The
+ * state, the next time step and the status counters are left as they were,
+ * so a run may be tuned between any two steps.
  * ms5 (may be NULL) receives the time per pass of each shape in that
  * order, best (may be NULL) two values: the chosen split and the fusion
  * flag. */

@@ -492,6 +492,34 @@ def test_autotune_picks_a_shape_and_keeps_the_state():
     assert np.array_equal(g.download(), U0)
 
 
+def test_autotune_between_steps_keeps_the_reference_time_step(ncpu):
+    """The tuner's timed passes fold CFL minima and status counts of their
+    scratch results into the control block; tuning between two steps must
+    leave the next step's dt (the CFL minimum of U) and the counters as they
+    were, so the run continues as the oracle's.  On a shock tube whose wave
+    speeds still grow, the scratch results' CFL minimum lies below U's."""
+    prob = problems.shock_tube(8)
+    o = oracle.from_problem(prob, threads=ncpu)
+    g = from_problem(prob)
+    try:
+        for _ in range(2):
+            o.step()
+            g.step()
+        before = g.status()
+        g.autotune(2)
+        after = g.status()
+        for f in ("pressure_floor", "density_floor", "zero_density", "nan_cells", "max_cool_loss"):
+            assert getattr(after, f) == getattr(before, f), f
+        for _ in range(2):
+            o.step()
+            s = g.step()
+            assert s.dt == pytest.approx(o.state.dt, rel=1e-12)
+        check(o, g, prob)
+    finally:
+        g.close()
+        o.close()
+
+
 @pytest.mark.parametrize("shape", ["default", "1-fused"])
 def test_colliding_winds_match_oracle(shape, ncpu):
     """Two spherical wind sources re-imposed before each stage (the

@@ -1315,6 +1315,13 @@ int wx3d_autotune(wx_ctx* c, int32_t reps, double* ms5, int32_t* best) {
     if ((rc = launch_dt(c, c->dU))) return rc;
     c->dt_valid = true;
   }
+  // The timed passes fold their CFL minima and status counts into the
+  // control block; it is saved here and put back after them, so that the
+  // next step takes the time step of U, as the reference does.
+  DevCtl saved;
+  WX_CUDA(cudaMemcpyAsync(c->hCtl, c->dCtl, sizeof(DevCtl), cudaMemcpyDeviceToHost, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
+  saved = *c->hCtl;
   cudaEvent_t e0, e1;
   WX_CUDA(cudaEventCreate(&e0));
   WX_CUDA(cudaEventCreate(&e1));
@@ -1354,6 +1361,9 @@ int wx3d_autotune(wx_ctx* c, int32_t reps, double* ms5, int32_t* best) {
   c->zsplit = bz;
   c->fuse = bf;
   if (rc) return rc;
+  *c->hCtl = saved;
+  WX_CUDA(cudaMemcpyAsync(c->dCtl, c->hCtl, sizeof(DevCtl), cudaMemcpyHostToDevice, c->stream));
+  WX_CUDA(cudaStreamSynchronize(c->stream));
   if (best) { best[0] = bz; best[1] = bf ? 1 : 0; }
   invalidate_graph(c);
   return WX_OK;
