@@ -78,6 +78,15 @@ Kern make_kern_lim(int lim) {
   return make_kern<NEQ, MHD, SOLVER, LIM_RUNTIME>();
 }
 
+// The source kernel compiled for the radiative runs' source terms
+// (EOS_H_RATE with COOL_H or COOL_TABLE) where the configuration has them.
+template <int NEQ>
+void pick_source_kernel(const wx_config& c, Kern& k) {
+  if (c.eos_type != WX_EOS_H_RATE || c.npassive < 1) return;
+  if (c.cooling_type == WX_COOL_H) k.src = source_kernel<NEQ, false, 1>;
+  if (c.cooling_type == WX_COOL_TABLE) k.src = source_kernel<NEQ, false, 2>;
+}
+
 // Supported combinations: hydro with 0..2 passives (HLL/HLL1/HLLC/LAX) and
 // ideal MHD without passives (HLL/HLL1/HLLE/HLLD/LAX).
 bool select_kern(const wx_config& c, Kern& k) {
@@ -90,8 +99,14 @@ bool select_kern(const wx_config& c, Kern& k) {
     const bool c_ = rs == WX_SOLVER_HLLC;
     switch (c.neqtot) {
       case 5: k = c_ ? make_kern_lim<5, false, WX_SOLVER_HLLC>(lim) : make_kern_lim<5, false, WX_SOLVER_HLL>(lim); return true;
-      case 6: k = c_ ? make_kern_lim<6, false, WX_SOLVER_HLLC>(lim) : make_kern_lim<6, false, WX_SOLVER_HLL>(lim); return true;
-      case 7: k = c_ ? make_kern_lim<7, false, WX_SOLVER_HLLC>(lim) : make_kern_lim<7, false, WX_SOLVER_HLL>(lim); return true;
+      case 6:
+        k = c_ ? make_kern_lim<6, false, WX_SOLVER_HLLC>(lim) : make_kern_lim<6, false, WX_SOLVER_HLL>(lim);
+        pick_source_kernel<6>(c, k);
+        return true;
+      case 7:
+        k = c_ ? make_kern_lim<7, false, WX_SOLVER_HLLC>(lim) : make_kern_lim<7, false, WX_SOLVER_HLL>(lim);
+        pick_source_kernel<7>(c, k);
+        return true;
       default: return false;
     }
   }

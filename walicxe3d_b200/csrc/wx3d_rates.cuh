@@ -11,11 +11,12 @@ namespace wx {
 constexpr double AMU = 1.660538782e-24;  // source/constants.f90:37
 constexpr double KB = 1.380650400e-16;   // source/constants.f90:38
 
-// calcTemp (hydro_core.f90:231-270)
-template <int FP>
+// calcTemp (hydro_core.f90:231-270); EOS >= 0 fixes the equation of state
+// at compile time, -1 reads it from ph.
+template <int FP, int EOS = -1>
 __device__ __forceinline__ double calc_temp(const double* p, const PhysParams& ph) {
   double temp = 0.0;
-  switch (ph.eos) {
+  switch (EOS >= 0 ? EOS : ph.eos) {
     case WX_EOS_ADIABATIC:
     case WX_EOS_SINGLE_SPECIE: temp = p[4] / p[0] * (ph.mu0 * AMU * ph.p_sc / ph.d_sc / KB); break;
     case WX_EOS_TWOTEMP:
@@ -175,7 +176,7 @@ __device__ __forceinline__ double get_lambda_schure(const double* __restrict__ T
 template <int FP>
 __device__ __forceinline__ void h_cool_step(double* u, double* p, double dts, const PhysParams& ph, double* mloss) {
   {
-    const double T = calc_temp<FP>(p, ph);
+    const double T = calc_temp<FP, WX_EOS_H_RATE>(p, ph);
     const double dh = p[0] / ph.mu0;
     const double y0 = p[FP] / dh;
     const double y1 = h_rate_y1(T, dh, y0, dts);
@@ -185,7 +186,7 @@ __device__ __forceinline__ void h_cool_step(double* u, double* p, double dts, co
   const double dh0 = p[FP];
   const double y0 = ph.mu0 * u[FP] / u[0];
   u[FP] = p[FP];
-  const double Temp = calc_temp<FP>(p, ph);
+  const double Temp = calc_temp<FP, WX_EOS_H_RATE>(p, ph);
   if (Temp > 1.e4) {
     const double L0 = aloss_h(y0, dh, dh0, Temp);
     const double ce = (2.0 * L0) / (3.0 * KB * dh * Temp);
@@ -204,14 +205,16 @@ __device__ __forceinline__ void h_cool_step(double* u, double* p, double dts, co
 // COOL_TABLE_METAL (apply_cooling, cooling.f90:303-369) and COOL_SCHURE
 // (cooling_schure.f90:134-228); updates p[4] and u[4] and folds the largest
 // fractional loss into mloss.  No-op for other cooling types or an unloaded
-// table.
-template <int NEQ, int FP>
+// table.  COOL and EOS >= 0 fix the cooling type and the equation of state
+// at compile time; -1 reads them from ph.
+template <int NEQ, int FP, int COOL = -1, int EOS = -1>
 __device__ __forceinline__ void table_cooling(double* u, double* p, double dts, const PhysParams& ph,
                                               const double* __restrict__ cool_lt, const double* __restrict__ cool_lc,
                                               int ncool, int nZ, double& mloss) {
-  if ((ph.cooling == WX_COOL_TABLE || ph.cooling == WX_COOL_TABLE_METAL) && ncool >= 2) {  // cooling.f90:303-369
-    const bool metal_tab = ph.cooling == WX_COOL_TABLE_METAL;
-    const double temp = calc_temp<FP>(p, ph);
+  const int cooling = COOL >= 0 ? COOL : ph.cooling;
+  if ((cooling == WX_COOL_TABLE || cooling == WX_COOL_TABLE_METAL) && ncool >= 2) {  // cooling.f90:303-369
+    const bool metal_tab = cooling == WX_COOL_TABLE_METAL;
+    const double temp = calc_temp<FP, EOS>(p, ph);
     const double logT = log10(temp);
     // metalpas = neqhydro + neqmhd + min(npassive, 1) (parameters.f90:318)
     const int mp = FP + (ph.npassive >= 1 ? 1 : 0) - 1;
@@ -238,8 +241,8 @@ __device__ __forceinline__ void table_cooling(double* u, double* p, double dts, 
       p[4] = p[4] * cf;
       u[4] = EK + ph.cv * p[4];
     }
-  } else if (ph.cooling == WX_COOL_SCHURE && ncool == 180) {  // cooling_schure.f90:134-228
-    const double T = calc_temp<FP>(p, ph);
+  } else if (cooling == WX_COOL_SCHURE && ncool == 180) {  // cooling_schure.f90:134-228
+    const double T = calc_temp<FP, EOS>(p, ph);
     if (T > 10.0) {
       const double Lambda0 = get_lambda_schure(cool_lt, cool_lc, T);
       const double dens = p[0] / ph.mu0;

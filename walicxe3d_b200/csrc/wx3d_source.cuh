@@ -28,11 +28,22 @@ struct SrcParams {
 
 // updatePrims + updateNeutralFraction + cooling for every physical cell
 // (main.f90:94-100), followed by the CFL minimum of the resulting PRIM.
-template <int NEQ, bool MHD>
-__global__ void __launch_bounds__(256) source_kernel(SrcParams P) {
+// Five CTAs per SM (at most 48 registers): the rate and loss formulas are
+// chains of dependent FP64 operations, and 40 resident warps hide them
+// better than the 24 that 80 registers allowed, spills included.  SPEC
+// fixes the source terms at compile time for the two combinations of the
+// radiative runs (1: EOS_H_RATE + COOL_H, 2: EOS_H_RATE + COOL_TABLE), which
+// leaves the other branches out of the register allocation; 0 reads the
+// equation of state and the cooling type from ph.
+template <int NEQ, bool MHD, int SPEC = 0>
+__global__ void __launch_bounds__(256, 5) source_kernel(SrcParams P) {
   constexpr int FP = MHD ? 8 : 5;
   constexpr bool HAS_PAS = NEQ > FP;
+  constexpr int EOS_C = SPEC ? WX_EOS_H_RATE : -1;
+  constexpr int COOL_C = SPEC == 1 ? WX_COOL_H : (SPEC == 2 ? WX_COOL_TABLE : -1);
   const PhysParams& ph = P.ph;
+  const int eos = EOS_C >= 0 ? EOS_C : ph.eos;
+  const int cooling = COOL_C >= 0 ? COOL_C : ph.cooling;
   const int t = threadIdx.x;
   const double dts = P.ctl->dt * ph.t_sc;
   const bool do_hrate = P.mode & 1, do_cool = P.mode & 2, use_prim = P.mode & 4, do_dt = P.mode & 8;
@@ -52,26 +63,26 @@ __global__ void __launch_bounds__(256) source_kernel(SrcParams P) {
         flow2prim<NEQ, MHD>(u, p, ph.inv_cv);
       }
       constexpr int fp = FP;
-      if (HAS_PAS && do_hrate && do_cool && ph.eos == WX_EOS_H_RATE && ph.cooling == WX_COOL_H) {
+      if (HAS_PAS && do_hrate && do_cool && eos == WX_EOS_H_RATE && cooling == WX_COOL_H) {
         h_cool_step<FP>(u, p, dts, ph, &mloss);  // hrate.f90:101-140 then cooling_h.f90:175-246
-      } else if (HAS_PAS && do_hrate && ph.eos == WX_EOS_H_RATE) {  // hrate.f90:101-140
-        const double T = calc_temp<FP>(p, ph);
+      } else if (HAS_PAS && do_hrate && eos == WX_EOS_H_RATE) {  // hrate.f90:101-140
+        const double T = calc_temp<FP, EOS_C>(p, ph);
         const double dh = p[0] / ph.mu0;
         const double y0 = p[fp] / dh;
         const double y1 = h_rate_y1(T, dh, y0, dts);
         p[fp] = p[0] * y1 / ph.mu0;
-        if (ph.cooling != WX_COOL_H) u[fp] = p[fp];
+        if (cooling != WX_COOL_H) u[fp] = p[fp];
       }
-      if (HAS_PAS && do_hrate && do_cool && ph.eos == WX_EOS_H_RATE && ph.cooling == WX_COOL_H) {
+      if (HAS_PAS && do_hrate && do_cool && eos == WX_EOS_H_RATE && cooling == WX_COOL_H) {
         // done above
-      } else if (do_cool && ph.cooling != WX_COOL_H) {  // cooling.f90:303-369, cooling_schure.f90:134-228
-        table_cooling<NEQ, FP>(u, p, dts, ph, P.cool_lt, P.cool_lc, P.ncool, P.nZ, mloss);
-      } else if (HAS_PAS && do_cool && ph.cooling == WX_COOL_H) {  // cooling_h.f90:175-246
+      } else if (do_cool && cooling != WX_COOL_H) {  // cooling.f90:303-369, cooling_schure.f90:134-228
+        table_cooling<NEQ, FP, COOL_C, EOS_C>(u, p, dts, ph, P.cool_lt, P.cool_lc, P.ncool, P.nZ, mloss);
+      } else if (HAS_PAS && do_cool && cooling == WX_COOL_H) {  // cooling_h.f90:175-246
         const double dh = p[0] / ph.mu0;
         const double dh0 = p[fp];
         const double y0 = ph.mu0 * u[fp] / u[0];
         u[fp] = p[fp];
-        const double Temp = calc_temp<FP>(p, ph);
+        const double Temp = calc_temp<FP, EOS_C>(p, ph);
         if (Temp > 1.e4) {
           const double L0 = aloss_h(y0, dh, dh0, Temp);
           const double ce = (2.0 * L0) / (3.0 * KB * dh * Temp);
