@@ -136,8 +136,7 @@ struct MarkParams {
 template <int NEQ, bool MHD>
 __global__ void __launch_bounds__(256, 4) mark_kernel(MarkParams P) {
   __shared__ double pp[3][18 * 18], pr[3][18 * 18];  // pressure and density, planes k-1..k+1
-  __shared__ int first_refine;                        // first cell (loop order) reaching refineThres
-  __shared__ double bmax;
+  __shared__ double bmax;                             // largest |delta|/value of the block
   __shared__ __align__(16) DevBlock B;                // the block's neighbour-table entry
   const int t = threadIdx.x;
   const int i = (t & 15) + 1, j = (t >> 4) + 1;
@@ -146,10 +145,9 @@ __global__ void __launch_bounds__(256, 4) mark_kernel(MarkParams P) {
     const int slot = P.work[w];
     __syncthreads();
     if (t < (int)(sizeof(DevBlock) / 4)) reinterpret_cast<int*>(&B)[t] = reinterpret_cast<const int*>(P.blocks + slot)[t];
-    if (t == 0) { first_refine = 0x7fffffff; bmax = 0.0; }
+    if (t == 0) bmax = 0.0;
     __syncthreads();
     double lmax = 0.0;
-    int lfirst = 0x7fffffff;
     // plane kk (0..17) is fetched into registers one plane ahead, then
     // converted into ring slot kk%3, so its loads overlap the gradients of
     // the plane before
@@ -214,33 +212,33 @@ __global__ void __launch_bounds__(256, 4) mark_kernel(MarkParams P) {
       if (k + 2 <= NC + 1) fetch(k + 2);
       __syncthreads();
       const int sm = (k - 1) % 3, sc = k % 3, sp = (k + 1) % 3;
-      const double dx2 = 2 * B.dx;
 #pragma unroll
       for (int v = 0; v < 2; ++v) {
         double (*a)[18 * 18] = v == 0 ? pp : pr;
-        // max over the axes of |delta|/c/dx2: correctly rounded division by
-        // the same positive c and dx2 is monotonic, so dividing the largest
-        // |delta| gives the reference's max of the three quotients bit for bit
+        // the reference's gradient of a cell is max over the axes of
+        // |delta|/c/(2 dx); correctly rounded division by the same positive
+        // c, and by the block's 2 dx, is monotonic, so the largest |delta|
+        // divided by c here, and the block's maximum of those divided by
+        // 2 dx once below, give its maximum gradient bit for bit
         const double c = a[sc][q(i, j)];
         const double dx_ = fabs(a[sc][q(i + 1, j)] - a[sc][q(i - 1, j)]);
         const double dy_ = fabs(a[sc][q(i, j + 1)] - a[sc][q(i, j - 1)]);
         const double dz_ = fabs(a[sp][q(i, j)] - a[sm][q(i, j)]);
-        const double gr = dmax(dmax(dx_, dy_), dz_) / c / dx2;
-        lmax = dmax(lmax, gr);
-        // reference loop order: i outer, j, k inner; pressure before density
-        const int order = (((i - 1) * NC + (j - 1)) * NC + (k - 1)) * 2 + v;
-        if (gr >= P.refine_thres && order < lfirst) lfirst = order;
+        lmax = dmax(lmax, dmax(dmax(dx_, dy_), dz_) / c);
       }
       __syncthreads();
     }
-    atomicMin(&first_refine, lfirst);
     for (int s = 16; s > 0; s >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, s));
     if ((t & 31) == 0) atomic_max_pos(reinterpret_cast<unsigned long long*>(&bmax), lmax);
     __syncthreads();
     if (t == 0) {
+      // the reference stops at the first cell whose gradient reaches
+      // refineThres (amr.f90:142-230): refinement depends only on whether
+      // the largest gradient does; coarsening on the largest gradient
+      const double gmax = bmax / (2 * B.dx);
       int flag;
-      if (first_refine != 0x7fffffff) flag = (B.level == P.maxlev) ? WX_FLAG_NONE : WX_FLAG_REFINE;
-      else flag = (bmax <= P.coarse_thres && B.level > 1) ? WX_FLAG_COARSE : WX_FLAG_NONE;
+      if (gmax >= P.refine_thres) flag = (B.level == P.maxlev) ? WX_FLAG_NONE : WX_FLAG_REFINE;
+      else flag = (gmax <= P.coarse_thres && B.level > 1) ? WX_FLAG_COARSE : WX_FLAG_NONE;
       P.flags[slot] = flag;
     }
   }
