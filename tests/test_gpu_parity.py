@@ -536,6 +536,45 @@ def test_colliding_winds_match_oracle(shape, ncpu):
     check(o, g, prob)
 
 
+WIND_EDGE_SEP = 1.0 - 18.0 / 128.0   # sources 9 finest cells (1/128 of the box) from the x boundaries
+
+
+def test_wind_spheres_next_to_the_domain_boundary_match_oracle(ncpu):
+    """Sources 9 finest cells from the x boundaries with spheres of 8: the
+    spheres reach the physical cells next to the boundary but not its ghost
+    layer.  The boundary ghosts then mirror those cells as they were before
+    the wind -- the reference fills them before userBoundary imposes it --
+    and the first stage reads them from U, not from the imposed copies."""
+    prob = problems.colliding_winds(nroot=2, maxlev=3, r_wind_cells=8, sep_pc=WIND_EDGE_SEP)
+    o = oracle.from_problem(prob, threads=ncpu)
+    g = from_problem(prob)
+    try:
+        for _ in range(6):
+            o.step()
+            g.step()
+        check(o, g, prob)
+    finally:
+        g.close()
+        o.close()
+
+
+def test_wind_sphere_through_the_domain_boundary_ghosts_is_refused():
+    """A sphere that reaches the ghost layer of the domain boundary would
+    need the wind at the ghosts' own positions, which mirroring a physical
+    cell does not give: refused, and the previous sources stay in force."""
+    from walicxe3d_b200._lib import WxError
+    prob = problems.colliding_winds(nroot=2, maxlev=3, r_wind_cells=8, sep_pc=WIND_EDGE_SEP)
+    g = from_problem(prob)
+    wider = [list(w) for w in prob.winds]
+    for w in wider:
+        w[6] *= 10.0 / 8.0                     # 10 finest cells: past the boundary 9 cells away
+    with pytest.raises(WxError) as e:
+        g.set_winds(wider)
+    assert e.value.code == 104
+    g.step()
+    g.close()
+
+
 def test_wind_sphere_on_a_level_transition_is_refused():
     """A sphere that reaches the ghost layer of a coarse/fine face would need
     the wind at ghost positions no same-level neighbour provides: refused."""

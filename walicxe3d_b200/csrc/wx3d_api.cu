@@ -260,6 +260,16 @@ struct wx_ctx {
   DevBlock* hblocks_next = nullptr;  // pinned buffer the next table is built in, then swapped in
   std::vector<double> hwind;      // wind sources, 12 doubles each (wx_wind)
   double* dWind = nullptr;
+  // Wind runs: the blocks a sphere reaches get a copy with the wind imposed
+  // in slots past max_blocks of dU, and the first stage gathers its ghosts
+  // through dBlocksWind, a neighbour table that points there.
+  int slot_cap = 0;                 // slots allocated in dU and dW
+  bool wind_ready = false;          // dBlocksWind and the lists match the mesh and the winds
+  int nwslot = 0;                   // reached blocks, copied each step
+  int wind_cap = 0;                 // entries allocated in the three arrays below
+  DevBlock* dBlocksWind = nullptr;  // [max_blocks + wind_cap]
+  int2* dWindPairs = nullptr;       // (slot, extra slot) of each reached block
+  int32_t* dWindWork = nullptr;     // the extra slots
   int nwork = 0;
   bool mesh_set = false;  // a mesh was set; it may hold no blocks (localBlocks all -1)
   int zsplit = 1;
@@ -373,9 +383,9 @@ void fill_phys(wx_ctx* c) {
 // Flags the blocks whose cells, ghost layers included, a wind sphere
 // reaches (cell centres from cellPos, amr.f90:1037-1065).  Returns false
 // (with the slot in *bad) if a sphere reaches the ghost layer of a face
-// with a coarser or finer neighbour: those ghosts would need the wind at
-// their own positions (or their sources the values before it), which only
-// a same-level neighbour provides.
+// with a coarser or finer neighbour, or of the domain boundary: those
+// ghosts would need the wind at their own positions (or their sources the
+// values before it), which only a same-level neighbour provides.
 bool flag_wind_blocks(const wx_ctx* c, DevBlock* hb, size_t n, int* bad) {
   const size_t nw = c->hwind.size() / 12;
   const double l_sc = c->cfg.l_sc;
@@ -402,7 +412,7 @@ bool flag_wind_blocks(const wx_ctx* c, DevBlock* hb, size_t n, int* bad) {
       if (!reach(W, lo, hi)) continue;
       b.wind = 1;
       for (int f = 0; f < 6; ++f) {
-        if (b.ftype[f] != WX_NEIGH_COARSER && b.ftype[f] != WX_NEIGH_FINER) continue;
+        if (b.ftype[f] != WX_NEIGH_COARSER && b.ftype[f] != WX_NEIGH_FINER && b.ftype[f] != WX_NEIGH_BOUNDARY) continue;
         const int ax = f / 2, side = f & 1;
         double glo[3], ghi[3];
         // the volume of the face's two ghost layers: it holds the ghost
@@ -468,18 +478,19 @@ int launch_dt(wx_ctx* c, const double* u) {
   return WX_OK;
 }
 
-int launch_wind(wx_ctx* c, double* u) {
+int launch_wind(wx_ctx* c, double* u, const DevBlock* blocks = nullptr, const int32_t* work = nullptr, int nwork = -1) {
   if (c->hwind.empty()) return WX_OK;
-  WindParams P{u, c->dBlocks, c->dWork, c->nwork, c->ph};
-  c->k.wind<<<grid_for(c, (const void*)c->k.wind, 256, 0, c->nwork), 256, 0, c->stream>>>(P);
+  if (nwork < 0) nwork = c->nwork;
+  WindParams P{u, blocks ? blocks : c->dBlocks, work ? work : c->dWork, nwork, c->ph};
+  c->k.wind<<<grid_for(c, (const void*)c->k.wind, 256, 0, nwork), 256, 0, c->stream>>>(P);
   WX_LAUNCHED();
   return WX_OK;
 }
 
 // fused: the corrector that also applies doViscousStep (whole blocks only)
 int launch_stage(wx_ctx* c, int order, const double* src, const double* base, double* out, double factor,
-                 bool fused = false, const double* gsrc = nullptr) {
-  StageParams P{src, base, out, c->dBlocks, c->dWork, c->nwork * c->zsplit, c->zsplit, c->dCtl, factor, c->ph,
+                 bool fused = false, const double* gsrc = nullptr, const DevBlock* blocks = nullptr) {
+  StageParams P{src, base, out, blocks ? blocks : c->dBlocks, c->dWork, c->nwork * c->zsplit, c->zsplit, c->dCtl, factor, c->ph,
                 sources_on(c) ? 0 : 1, gsrc ? gsrc : src, order == 1 && c->g_step ? c->dG : nullptr};
   auto fn = order == 1 ? c->k.stage1 : (fused ? c->k.stage2v : c->k.stage2);
   const size_t smem = order == 1 ? c->k.smem1 : (fused ? c->k.smem2v : c->k.smem2);
@@ -560,22 +571,30 @@ int enqueue_solver(wx_ctx* c, bool bump_it, bool finish_output) {
   WX_LAUNCHED();
   int rc;
   if (!c->hwind.empty()) {
+    if (!c->wind_ready) return fail(c, WX_ERR_GENERIC, "wind sources without their redirected neighbour table");
     // Wind run (userBoundary after every ghost fill, winds.f90:123-240).
     // Stage 1 of godunov.f90 refreshes only the ghost primitives after
     // boundary(1, U): the physical cells feed their fluxes with the
-    // primitives of U before the wind, the ghosts see it.  So the physical
-    // cells come from U and the ghosts from a wind-imposed copy of U in W,
-    // which is also the base of stage 2; boundary(2, UP) imposes the wind on
-    // UP's physical cells.  The result goes to U (no swap).
-    WX_CUDA(cudaMemcpyAsync(c->dW, c->dU, sizeof(double) * (size_t)c->max_blocks * c->neq * BCELLS,
-                            cudaMemcpyDeviceToDevice, c->stream));
-    if ((rc = launch_wind(c, c->dW))) return rc;
-    if ((rc = launch_stage(c, 1, c->dU, c->dU, c->dUP, 0.5, false, c->dW))) return rc;
+    // primitives of U before the wind, the ghosts see it.  The blocks a
+    // sphere reaches are copied into extra slots and take the wind there;
+    // stage 1 reads its own cells from U and gathers its ghosts through
+    // dBlocksWind, which points at those copies.  Then U takes the wind in
+    // place and is the base of stage 2; boundary(2, UP) imposes the wind on
+    // UP's physical cells.  The result goes to W and the buffers swap.
+    if (c->nwslot > 0) {
+      copy_slots_kernel<<<dim3(16, c->nwslot), 256, 0, c->stream>>>(c->dU, c->dWindPairs, c->neq);
+      WX_LAUNCHED();
+      if ((rc = launch_wind(c, c->dU, c->dBlocksWind, c->dWindWork, c->nwslot))) return rc;
+    }
+    if ((rc = launch_stage(c, 1, c->dU, c->dU, c->dUP, 0.5, false, nullptr, c->nwslot > 0 ? c->dBlocksWind : nullptr)))
+      return rc;
     if ((rc = launch_wind(c, c->dUP))) return rc;
-    if ((rc = launch_stage(c, 2, c->dUP, c->dW, c->dU, 1.0, fuse_visc(c)))) return rc;
-    if (!fuse_visc(c) && (rc = launch_visc(c, 0, c->dU))) return rc;
+    if ((rc = launch_wind(c, c->dU))) return rc;
+    if ((rc = launch_stage(c, 2, c->dUP, c->dU, c->dW, 1.0, fuse_visc(c)))) return rc;
+    if (!fuse_visc(c) && (rc = launch_visc(c, 0, c->dW))) return rc;
     step_end_kernel<<<1, 1, 0, c->stream>>>(c->dCtl, finish_output ? 1 : 0);
     WX_LAUNCHED();
+    std::swap(c->dU, c->dW);
     c->prestep = true;
     c->g_valid = false;
     c->dt_valid = !src;
@@ -766,6 +785,7 @@ int wx3d_init(const wx_config* cfg, int32_t max_blocks, wx_ctx** out) {
   if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) return cleanup(WX_ERR_CUDA);
   c->stream = c->own;
   if (cudaMalloc(&c->dU, n * 8) || cudaMalloc(&c->dUP, n * 8) || cudaMalloc(&c->dW, n * 8)) return cleanup(WX_ERR_CUDA);
+  c->slot_cap = max_blocks;
   cudaMemset(c->dU, 0, n * 8);
   cudaMemset(c->dUP, 0, n * 8);
   cudaMemset(c->dW, 0, n * 8);
@@ -797,6 +817,7 @@ int wx3d_finalize(wx_ctx* c) {
   cudaFree(c->dBlocks); cudaFree(c->dWork); cudaFree(c->dFlags); cudaFree(c->dCtl); cudaFree(c->dCool);
   cudaFree(c->dTrust);
   cudaFree(c->dWind);
+  cudaFree(c->dBlocksWind); cudaFree(c->dWindPairs); cudaFree(c->dWindWork);
   cudaFree(c->dOps);
   cudaFree(c->dItems);
   cudaFree(c->dG);
@@ -928,8 +949,8 @@ static int build_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nhal
   }
   int bad = -1;
   if (!flag_wind_blocks(c, hb, c->max_blocks, &bad))
-    return fail(c, WX_ERR_UNSUPPORTED, "slot %d: a wind sphere reaches the ghost layer of a coarse/fine face; "
-                "refine the zone around the source (refineZone) further", bad);
+    return fail(c, WX_ERR_UNSUPPORTED, "slot %d: a wind sphere reaches the ghost layer of a coarse/fine face or of the domain "
+                "boundary; refine the zone around the source (refineZone) further", bad);
   return WX_OK;
 }
 
@@ -1107,6 +1128,94 @@ static int sync_host_table(wx_ctx* c) {
   return WX_OK;
 }
 
+// Wind runs: lists the occupied blocks a sphere reaches, gives each an
+// extra slot past max_blocks in dU and dW (growing both when needed), and
+// builds dBlocksWind, the neighbour table whose same-level, coarser and
+// finer entries point at the extra slot of a reached block.  Domain-boundary
+// ghosts keep mirroring the block's own cells before the wind, as the
+// reference's fill does before userBoundary (spheres that reach those
+// ghosts are refused by flag_wind_blocks).
+static int prepare_wind_redirect(wx_ctx* c) {
+  c->wind_ready = false;
+  c->nwslot = 0;
+  if (c->hwind.empty() || !c->mesh_set) return WX_OK;
+  int rc = sync_host_table(c);
+  if (rc) return rc;
+  const DevBlock* hb = c->hblocks;
+  std::vector<int32_t> reached;
+  for (int s : c->work)
+    if (hb[s].wind) reached.push_back(s);
+  const int nr = (int)reached.size();
+  const int mb = c->max_blocks;
+  if (mb + nr > c->slot_cap) {
+    const int cap = mb + std::max(nr, 64);
+    const size_t per = (size_t)c->neq * BCELLS * 8;
+    double *u = nullptr, *w = nullptr;
+    WX_CUDA(cudaStreamSynchronize(c->stream));
+    if (cudaMalloc(&u, per * cap) != cudaSuccess || cudaMalloc(&w, per * cap) != cudaSuccess) {
+      cudaFree(u);
+      return fail(c, WX_ERR_CUDA, "wind: no device memory for %d extra slots", cap - mb);
+    }
+    WX_CUDA(cudaMemcpy(u, c->dU, per * mb, cudaMemcpyDeviceToDevice));
+    WX_CUDA(cudaMemset(w, 0, per * cap));
+    cudaFree(c->dU);
+    cudaFree(c->dW);
+    c->dU = u;
+    c->dW = w;
+    c->slot_cap = cap;
+    c->prestep = false;
+    c->g_valid = false;
+    invalidate_graph(c);
+  }
+  if (nr > c->wind_cap) {
+    const int cap = std::max(nr, 64);
+    cudaFree(c->dBlocksWind);
+    cudaFree(c->dWindPairs);
+    cudaFree(c->dWindWork);
+    c->dBlocksWind = nullptr;
+    c->dWindPairs = nullptr;
+    c->dWindWork = nullptr;
+    c->wind_cap = 0;
+    if (cudaMalloc(&c->dBlocksWind, sizeof(DevBlock) * (size_t)(mb + cap)) != cudaSuccess ||
+        cudaMalloc(&c->dWindPairs, sizeof(int2) * (size_t)cap) != cudaSuccess ||
+        cudaMalloc(&c->dWindWork, sizeof(int32_t) * (size_t)cap) != cudaSuccess)
+      return fail(c, WX_ERR_CUDA, "wind: no device memory for the redirected table");
+    c->wind_cap = cap;
+  }
+  std::vector<int32_t> extra(mb, -1);
+  std::vector<int2> pairs(nr);
+  std::vector<int32_t> ework(nr);
+  for (int r = 0; r < nr; ++r) {
+    extra[reached[r]] = mb + r;
+    pairs[r] = make_int2(reached[r], mb + r);
+    ework[r] = mb + r;
+  }
+  std::vector<DevBlock> tab(hb, hb + mb);
+  tab.resize((size_t)mb + nr);
+  for (int s = 0; s < mb; ++s) {
+    DevBlock& b = tab[s];
+    if (b.level < 1) continue;
+    for (int f = 0; f < 6; ++f) {
+      const int t = b.ftype[f];
+      const int nq = t == WX_NEIGH_FINER ? 4 : ((t == WX_NEIGH_SAME || t == WX_NEIGH_COARSER) ? 1 : 0);
+      for (int q = 0; q < nq; ++q) {
+        const int nbs = b.fnb[f][q];
+        if (nbs >= 0 && nbs < mb && extra[nbs] >= 0) b.fnb[f][q] = extra[nbs];
+      }
+    }
+  }
+  for (int r = 0; r < nr; ++r) tab[(size_t)mb + r] = hb[reached[r]];
+  WX_CUDA(cudaMemcpy(c->dBlocksWind, tab.data(), sizeof(DevBlock) * tab.size(), cudaMemcpyHostToDevice));
+  if (nr > 0) {
+    WX_CUDA(cudaMemcpy(c->dWindPairs, pairs.data(), sizeof(int2) * nr, cudaMemcpyHostToDevice));
+    WX_CUDA(cudaMemcpy(c->dWindWork, ework.data(), sizeof(int32_t) * nr, cudaMemcpyHostToDevice));
+  }
+  c->nwslot = nr;
+  c->wind_ready = true;
+  invalidate_graph(c);
+  return WX_OK;
+}
+
 // Makes the mesh that build_mesh left in hblocks_next the context's.
 static int commit_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nhalo, std::vector<int32_t>& work) {
   c->local.assign(c->max_blocks, -1);
@@ -1134,7 +1243,7 @@ static int commit_mesh(wx_ctx* c, int32_t nslots, const int32_t* lb, int32_t nha
   c->prestep = false;
   c->g_valid = false;
   invalidate_graph(c);
-  return WX_OK;
+  return prepare_wind_redirect(c);
 }
 
 // The device build serves meshes without halo slots or wind sources.
@@ -1186,8 +1295,8 @@ int wx3d_set_winds(wx_ctx* c, int32_t nwind, const wx_wind* winds) {
   std::memcpy(hb, c->hblocks, sizeof(DevBlock) * (size_t)c->max_blocks);
   if (!flag_wind_blocks(c, hb, c->max_blocks, &bad)) {
     c->hwind = prev;
-    return fail(c, WX_ERR_UNSUPPORTED, "slot %d: a wind sphere reaches the ghost layer of a coarse/fine face; "
-                "refine the zone around the source (refineZone) further", bad);
+    return fail(c, WX_ERR_UNSUPPORTED, "slot %d: a wind sphere reaches the ghost layer of a coarse/fine face or of the domain "
+                "boundary; refine the zone around the source (refineZone) further", bad);
   }
   WX_CUDA(cudaStreamSynchronize(c->stream));
   cudaFree(c->dWind);
@@ -1202,7 +1311,7 @@ int wx3d_set_winds(wx_ctx* c, int32_t nwind, const wx_wind* winds) {
                           c->stream));
   WX_CUDA(cudaStreamSynchronize(c->stream));
   invalidate_graph(c);
-  return WX_OK;
+  return prepare_wind_redirect(c);
 }
 
 int wx3d_step_part(wx_ctx* c, int32_t part) {

@@ -767,6 +767,17 @@ struct WindParams {
   PhysParams ph;
 };
 
+// Copies whole blocks within one array: slot pairs (from, to), one row of
+// CTAs per pair.
+__global__ void copy_slots_kernel(double* u, const int2* __restrict__ pairs, int neq) {
+  const int2 pr = pairs[blockIdx.y];
+  const size_t n = (size_t)neq * BCELLS;
+  const double* from = u + (size_t)pr.x * n;
+  double* to = u + (size_t)pr.y * n;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+    to[c] = from[c];
+}
+
 template <int NEQ, bool MHD>
 __global__ void __launch_bounds__(256) wind_kernel(WindParams P) {
   for (int w = blockIdx.x; w < P.nwork; w += gridDim.x) {
