@@ -205,7 +205,10 @@ typedef struct wx_wind {
  * the r^-2 wind in all cells, ghosts included, within a source's radius.
  * The library applies it where the stages read those cells.  nwind = 0
  * removes the sources.  The zone refinement the reference does at it = 0
- * (refineZone) is the host's, like the rest of the mesh. */
+ * (refineZone) is the host's, like the rest of the mesh.  A sphere that
+ * reaches the ghost layer of a coarse/fine face or of the domain boundary
+ * is refused (WX_ERR_UNSUPPORTED, the previous sources stay), here and in
+ * wx3d_set_mesh / wx3d_admesh. */
 int wx3d_set_winds(wx_ctx* ctx, int32_t nwind, const wx_wind* winds);
 
 /* With fusion on (the default) and whole blocks per CTA (zsplit 1), the
