@@ -582,8 +582,11 @@ int enqueue_solver(wx_ctx* c, bool bump_it, bool finish_output) {
     // place and is the base of stage 2; boundary(2, UP) imposes the wind on
     // UP's physical cells.  The result goes to W and the buffers swap.
     if (c->nwslot > 0) {
-      copy_slots_kernel<<<dim3(16, c->nwslot), 256, 0, c->stream>>>(c->dU, c->dWindPairs, c->neq);
-      WX_LAUNCHED();
+      for (int r = 0; r < c->nwslot; r += 65535) {  // grid y limit
+        copy_slots_kernel<<<dim3(16, std::min(65535, c->nwslot - r)), 256, 0, c->stream>>>(c->dU, c->dWindPairs + r,
+                                                                                          c->neq);
+        WX_LAUNCHED();
+      }
       if ((rc = launch_wind(c, c->dU, c->dBlocksWind, c->dWindWork, c->nwslot))) return rc;
     }
     if ((rc = launch_stage(c, 1, c->dU, c->dU, c->dUP, 0.5, false, nullptr, c->nwslot > 0 ? c->dBlocksWind : nullptr)))
