@@ -1,6 +1,6 @@
 """Physics pins of the CPU oracle (the reference ships no golden data):
 exact Riemann solutions, FP64 conservation, symmetry, Brio-Wu structure,
-the hrate rate equation and the table-cooling loss law."""
+the hrate rate equation, the table-cooling loss law and the imposed wind."""
 import numpy as np
 import pytest
 
@@ -307,3 +307,43 @@ def test_table_cooling_removes_n2_lambda_of_the_thermal_energy(ncpu):
         assert maxloss == pytest.approx((1.0 - np.exp(-x)).max(), rel=1e-12)
         if dt_yr > 1e3:
             assert np.any(np.exp(-x) < 1.0 - cfg.cooling_limit)
+
+
+def test_imposed_wind_carries_the_mass_loss_rate(ncpu):
+    """imposeSphericalWind (winds.f90:123-240) writes a free r^-2 wind in every
+    cell whose centre lies within a source's radius.  A pin of the
+    restatement's geometry (cellPos, amr.f90:1037-1065) and unit scalings:
+    after one ghost exchange the physical cells inside a sphere carry, in
+    cgs, a radial mass flux 4 pi r^2 rho v_r equal to the source's Mdot, the
+    terminal speed, and the wind temperature (p = rho k T / (mu m_u)); every
+    other cell is as it was."""
+    from walicxe3d_b200.mesh import cell_centres
+
+    prob = problems.colliding_winds(nroot=2, maxlev=3, r_wind_cells=8)
+    o = oracle.from_problem(prob, threads=ncpu)
+    o.boundary(2, oracle.U_)
+    o.update_prims()
+    P = o.PRIM[: prob.nblocks]
+    U = o.U[: prob.nblocks]
+    o.close()
+    cfg = prob.cfg
+    xyz = cell_centres(cfg, prob.tree, [int(b) for b in prob.local_blocks]) * cfg.l_sc   # cm
+    inside = np.zeros(P[:, 0].shape, bool)
+    for w in prob.winds:
+        xc, yc, zc, radius, mdot, vinf, temp, mu = w[0], w[1], w[2], w[6], w[7], w[8], w[9], w[10]
+        d = np.stack([xyz[:, 0] - xc, xyz[:, 1] - yc, xyz[:, 2] - zc])
+        r = np.sqrt((d ** 2).sum(axis=0))
+        m = r < radius
+        assert m.sum() > 100
+        inside |= m
+        rho = P[:, 0][m] * cfg.d_sc
+        v = np.stack([P[:, 1 + a][m] for a in range(3)]) * cfg.v_sc
+        rhat = d[:, m] / r[m]
+        vr = (v * rhat).sum(axis=0)
+        assert np.allclose(4.0 * np.pi * r[m] ** 2 * rho * vr, mdot, rtol=1e-12, atol=0)
+        assert np.allclose(vr, vinf, rtol=1e-12, atol=0)
+        assert np.abs(v - vr * rhat).max() <= 1e-9 * vinf            # no transverse velocity
+        T = P[:, 4][m] * cfg.p_sc * mu * C.AMU / (rho * C.KB)
+        assert np.allclose(T, temp, rtol=1e-9, atol=0)
+    outside = np.broadcast_to(~inside[:, None], U.shape)
+    assert np.array_equal(U[outside], prob.U[outside])
