@@ -7,6 +7,7 @@ import pytest
 import oracle
 from walicxe3d_b200 import config as C
 from walicxe3d_b200 import problems
+from walicxe3d_b200.mesh import cell_centres
 
 from exact_riemann import sample
 
@@ -317,8 +318,6 @@ def test_imposed_wind_carries_the_mass_loss_rate(ncpu):
     cgs, a radial mass flux 4 pi r^2 rho v_r equal to the source's Mdot, the
     terminal speed, and the wind temperature (p = rho k T / (mu m_u)); every
     other cell is as it was."""
-    from walicxe3d_b200.mesh import cell_centres
-
     prob = problems.colliding_winds(nroot=2, maxlev=3, r_wind_cells=8)
     o = oracle.from_problem(prob, threads=ncpu)
     o.boundary(2, oracle.U_)
@@ -347,3 +346,43 @@ def test_imposed_wind_carries_the_mass_loss_rate(ncpu):
         assert np.allclose(T, temp, rtol=1e-9, atol=0)
     outside = np.broadcast_to(~inside[:, None], U.shape)
     assert np.array_equal(U[outside], prob.U[outside])
+
+
+def test_sedov_taylor_blast_radius_on_the_oracle(ncpu):
+    """The oracle on the Sedov-Taylor point blast (gamma = 5/3, E = rho = 1,
+    eta = 0) at 32^3 and 64^3 cells: at the output time where the
+    similarity solution R = xi0 (E t^2/rho)^(1/5), xi0 = 1.15167, reaches 0.3,
+    the shell-averaged shock radius approaches it as the mesh is refined
+    (7.2 % then 4.3 % here; the GPU test carries the same check to 256^3)
+    and the peak density rises towards the strong-shock limit 4."""
+    xi0, r_target = 1.15167, 0.3
+    t_target = (r_target / xi0) ** 2.5
+    errs, peaks = [], []
+    for nroot in (2, 4):
+        prob = problems.sedov(nroot, radius_cells=3.0)
+        prob.cfg.visc_eta = 0.0
+        prob.cfg.dtout = t_target
+        o = oracle.from_problem(prob, threads=ncpu)
+        for _ in range(2000):
+            o.step()
+            if o.state.nextout > 1:     # the step that met the output time
+                break
+        assert o.state.time == pytest.approx(t_target, rel=1e-14)
+        U = o.U[: prob.nblocks]
+        o.close()
+        n = nroot * 16
+        xyz = cell_centres(prob.cfg, prob.tree, [int(b) for b in prob.local_blocks])
+        r = np.sqrt(((xyz - 0.5) ** 2).sum(axis=1)).ravel()
+        idx = np.minimum((r * n).astype(np.int64), n // 2)
+        ok = idx < n // 2
+        prof = np.bincount(idx[ok], weights=U[:, 0].ravel()[ok], minlength=n // 2) / np.maximum(
+            np.bincount(idx[ok], minlength=n // 2), 1)
+        rc = (np.arange(n // 2) + 0.5) / n
+        ip = int(np.argmax(prof))
+        half = 0.5 * (1.0 + prof[ip])
+        j = ip + int(np.argmax(prof[ip:] < half))
+        r_shock = rc[j - 1] + (half - prof[j - 1]) / (prof[j] - prof[j - 1]) * (rc[j] - rc[j - 1])
+        errs.append(abs(r_shock / r_target - 1.0))
+        peaks.append(prof[ip])
+    assert errs[1] < errs[0] and errs[1] < 0.05, errs
+    assert peaks[0] < peaks[1] < 4.0, peaks
