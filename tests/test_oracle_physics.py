@@ -386,3 +386,37 @@ def test_sedov_taylor_blast_radius_on_the_oracle(ncpu):
         peaks.append(prof[ip])
     assert errs[1] < errs[0] and errs[1] < 0.05, errs
     assert peaks[0] < peaks[1] < 4.0, peaks
+
+
+def test_viscous_step_damps_a_cosine_mode_by_its_eigenvalue(ncpu):
+    """doViscousStep (hydro_solver.f90:217-250) adds eta times the 7-point
+    Laplacian of the stage result.  On a density wave at rest in uniform
+    pressure -- a stationary contact, which the HLLC fluxes leave in place --
+    with reflective walls, rho = 1 + a cos(pi x / L) sampled at the cell
+    centres is an eigenvector of that Laplacian (the walls mirror the
+    cells), so one step multiplies a by 1 + eta (2 cos(pi/N) - 2), N cells
+    across, whatever dt is.  32^3 cells on 2^3 blocks, so the wave crosses
+    the block faces, whose ghosts come from the half-step state."""
+    eta, amp, N = 0.05, 0.1, 32
+    cfg = C.Config(solver_type=C.SOLVER_HLLC, limiter_type=C.LIMITER_MINMOD, nbroot=(2, 2, 2), maxlev=1,
+                   gamma=5.0 / 3.0, cfl=0.4, visc_eta=eta, bc=(C.BC_REFLECTIVE,) * 6)
+    tree = problems.BlockTree(cfg.nbroot, 1).roots()
+
+    def prim_fn(xyz):
+        prim = np.zeros((xyz.shape[0], cfg.neqtot) + xyz.shape[2:])
+        prim[:, 0] = 1.0 + amp * np.cos(np.pi * xyz[:, 0])
+        prim[:, 4] = 1.0
+        return prim
+
+    prob = problems._finish("viscous-mode", cfg, tree, prim_fn, 1)
+    o = oracle.from_problem(prob, threads=ncpu)
+    for _ in range(3):
+        o.step()
+    U = o.U[: prob.nblocks]
+    o.close()
+    xyz = cell_centres(cfg, tree, [int(b) for b in prob.local_blocks])
+    mode = np.cos(np.pi * xyz[:, 0])
+    g = 1.0 + eta * (2.0 * np.cos(np.pi / N) - 2.0)
+    assert np.abs(U[:, 0] - (1.0 + amp * g ** 3 * mode)).max() < 1e-13
+    assert np.abs(U[:, 1:4]).max() < 1e-13              # still at rest
+    assert np.abs(U[:, 4] - 1.0 / (cfg.gamma - 1.0)).max() < 1e-13   # uniform energy stays uniform
